@@ -1,0 +1,222 @@
+/*
+ * rigidfibers.h - C ABI of the B200-native rigid-fiber slender-body solver.
+ *
+ * One handle owns one simulation on one GPU: the fiber state (triple-buffered
+ * positions and orientations, double-buffered velocities), the dense system
+ * A x = b, the Krylov workspace and the preconditioner.  Every entry point is
+ * synchronous at return, takes and returns plain host pointers, and reports a
+ * status code; none calls exit().  Handles are independent (one CUDA stream
+ * each) and may be used from different host threads; one handle must not be
+ * used from two threads at once.
+ *
+ * Reference interface that each entry point replaces (paths inside
+ * ericwolter/rigidfibers_kth):
+ *   Simulation(Configuration)          src/simulation.h:39, src/simulation.cu:40-53
+ *   Simulation::step(size_t)           src/simulation.h:42, src/simulation.cu:279-301
+ *   Simulation::assembleSystem()       src/simulation.h:79, src/simulation.cu:303-322
+ *   Simulation::solveSystem()          src/simulation.h:80, src/simulation.cu:324-351
+ *   Simulation::updateVelocities()     src/simulation.h:81, src/simulation.cu:353-384
+ *   Simulation::updateFibers(bool)     src/simulation.h:82, src/simulation.cu:386-424
+ *   FiberParams                        src/common.h:49-68
+ *   Parameters::parse*File             src/parameters.cc:24-227
+ * and the Fortran boundary solve_coeffs*_ / compute_velocities*
+ * (fortran/coeffs_and_vels.f90:10-746) that the same calls cover.
+ *
+ * Index conventions (identical to the reference):
+ *   fiber state      double[3*M], (x,y,z) of fiber 0, then fiber 1, ...
+ *   coefficients     n = 3*N*M, index (i*N + k)*3 + d   (fiber i, term k+1, axis d)
+ *   system matrix    n x n column-major, A[row + col*n]
+ */
+#ifndef RIGIDFIBERS_H_
+#define RIGIDFIBERS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* every declaration below is exported from librigidfibers.so */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define RF_ABI_VERSION 1
+
+typedef enum rf_status {
+    RF_OK = 0,
+    RF_ERR_INVALID_ARG = 1,   /* bad size, null pointer, unsupported option */
+    RF_ERR_OOM = 2,           /* device allocation failed */
+    RF_ERR_CUDA = 3,          /* CUDA runtime error; see rf_last_error() */
+    RF_ERR_NOT_CONVERGED = 4, /* GMRES budget spent above tolerance (state still advanced) */
+    RF_ERR_DEVICE_TIMEOUT = 5,/* a bounded device wait gave up */
+    RF_ERR_NAN = 6,           /* non-finite value in inputs or results */
+    RF_ERR_NO_DEVICE = 7      /* no CUDA device / driver */
+} rf_status;
+
+/* Storage precision of A and arithmetic of the solve. */
+typedef enum rf_precision {
+    RF_PREC_FP64 = 0,        /* plain method: FP64 assembly, FP64 A, FP64 GMRES */
+    RF_PREC_FP32 = 1,        /* plain method in FP32 (reference "float" build) */
+    RF_PREC_MIXED_BF16 = 2,  /* BF16 A for inner GMRES (FP32 accumulate), FP32 A for FP64-residual refinement */
+    RF_PREC_MIXED_FP32 = 3   /* FP32 A for inner GMRES and for the FP64-residual refinement */
+} rf_precision;
+
+typedef enum rf_preconditioner {
+    RF_PC_NONE = 0,          /* block-Jacobi on the fiber's own 15x15 block == identity here */
+    RF_PC_CLUSTER = 1,       /* exact fiber block of the inverse of its k-NN cluster submatrix */
+    RF_PC_LEARNED = 2        /* MLP-corrected block (see rf_pc_* below); falls back to RF_PC_NONE */
+} rf_preconditioner;
+
+typedef enum rf_velocity_mode {
+    RF_VEL_RECOMPUTE = 0,    /* re-evaluate the pair integrals with the solved forces (reference) */
+    RF_VEL_REUSE = 1         /* reuse P0/P1 projections stored during assembly (two GEMVs) */
+} rf_velocity_mode;
+
+/* Run parameters.  The first eight fields mirror FiberParams
+ * (src/common.h:49-68) and the positional run*.in file
+ * (src/parameters.cc:124-180, fortran/advect_fibers.f90:182-222). */
+typedef struct rf_params {
+    double slenderness;                  /* epsilon (e.g. 0.01) */
+    double timestep;                     /* dt (e.g. 0.1) */
+    int32_t num_fibers;                  /* M */
+    int32_t num_timesteps;               /* informational; rf_step is called by the caller */
+    int32_t num_terms_in_force_expansion;/* N, 1..8 */
+    int32_t num_quadrature_intervals;    /* NoQI, 1..16; 3 Gauss points each */
+    int32_t use_analytical_integration;  /* 1: analytic inner integral, 0: Gauss quadrature */
+    int32_t use_direct_solver;           /* 1: dense LU on the device, 0: GMRES */
+    int32_t gmres_restart;               /* restart length (run100_iter.in: 10) */
+    int32_t gmres_max_iters;             /* iteration budget (100) */
+    double gmres_tol;                    /* ||b - A x|| / ||b|| target (1e-5) */
+    double external_force[3];            /* per-fiber external force (0, 0, -1) */
+    int32_t precision;                   /* rf_precision */
+    int32_t preconditioner;              /* rf_preconditioner */
+    int32_t velocity_mode;               /* rf_velocity_mode */
+    int32_t device;                      /* CUDA device ordinal */
+    int32_t max_refinements;             /* mixed precision: outer refinement steps (default 30) */
+    int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 12) */
+    double inner_tol;                    /* mixed precision: inner GMRES relative tolerance (default 1e-3) */
+    double near_field_c;                 /* mixed precision: squared distance below which the analytic
+                                            integral stays FP64 (default 10, the recursion switch) */
+    int32_t reserved[8];
+} rf_params;
+
+/* GMRES / refinement statistics of the last solve. */
+typedef struct rf_solve_stats {
+    int32_t converged;        /* 1 if ||b-Ax||/||b|| <= tol */
+    int32_t iterations;       /* Arnoldi steps (inner steps summed for mixed precision) */
+    int32_t matvecs;          /* low- or full-precision matvecs */
+    int32_t refinements;      /* outer FP64-residual refinements (mixed precision) */
+    double residual;          /* final true ||b-Ax||/||b|| */
+    double seconds;           /* device time of the solve */
+} rf_solve_stats;
+
+typedef struct rf_handle rf_handle;
+
+/* Fill *p with the reference defaults (run100_iter.in with eps 0.01). */
+void rf_params_default(rf_params *p);
+
+/* Simulation(Configuration): allocate device state for p->num_fibers fibers and
+ * upload the initial layout.  Orientations are normalised (as the Fortran
+ * driver does, advect_fibers.f90:332-340). */
+rf_status rf_create(const rf_params *p, const double *positions, const double *orientations,
+                    rf_handle **out);
+rf_status rf_destroy(rf_handle *h);
+
+/* Simulation::step: assemble, solve, velocities, advect (Euler if
+ * current_timestep == 0, else the second-order multistep), then rotate the
+ * state buffers. */
+rf_status rf_step(rf_handle *h, size_t current_timestep);
+/* The four phases of step, callable one by one. */
+rf_status rf_assemble_system(rf_handle *h);
+rf_status rf_solve_system(rf_handle *h);
+rf_status rf_update_velocities(rf_handle *h);
+/* Advects the fibers and rotates the triple/double buffers. */
+rf_status rf_update_fibers(rf_handle *h, int first_timestep);
+
+/* State access (host buffers of 3*M doubles). */
+rf_status rf_get_state(rf_handle *h, double *positions, double *orientations);
+rf_status rf_set_state(rf_handle *h, const double *positions, const double *orientations);
+rf_status rf_get_velocities(rf_handle *h, double *translational, double *rotational);
+/* Coefficient vector (n doubles) and right-hand side (n doubles). */
+rf_status rf_get_coeffs(rf_handle *h, double *x);
+rf_status rf_get_rhs(rf_handle *h, double *b);
+/* Dense matrix, n*n doubles column-major (converted from the stored precision). */
+rf_status rf_get_matrix(rf_handle *h, double *A);
+/* y = A x with the stored matrix (FP64 host vectors of n doubles). */
+rf_status rf_matvec(rf_handle *h, const double *x, double *y);
+rf_status rf_get_solve_stats(rf_handle *h, rf_solve_stats *s);
+/* Multistep history for checkpoint/resume: previous positions/orientations
+ * and previous velocities (3*M doubles each). */
+rf_status rf_get_history(rf_handle *h, double *prev_pos, double *prev_orient, double *prev_vel,
+                         double *prev_rot);
+rf_status rf_set_history(rf_handle *h, const double *prev_pos, const double *prev_orient,
+                         const double *prev_vel, const double *prev_rot, const double *coeffs);
+
+/* Sizes. */
+int64_t rf_system_size(const rf_handle *h);   /* n = 3*N*M */
+int64_t rf_matrix_ld(const rf_handle *h);     /* leading dimension of the stored A */
+/* CUDA stream (cudaStream_t) the handle launches on; for event timing. */
+void *rf_get_stream(rf_handle *h);
+/* Number of kernels the handle has launched since creation. */
+int64_t rf_kernel_launches(const rf_handle *h);
+/* Last error message of the handle (or of the last failed rf_create if h is NULL). */
+const char *rf_last_error(const rf_handle *h);
+const char *rf_status_string(rf_status s);
+
+/* ---- Seeded synthetic layouts -------------------------------------------
+ * Centres by rejection sampling (minimum centre distance min_dist), either
+ * uniform in the cube [0, box]^3 (distribution 0) or isotropic Gaussian with
+ * standard deviation box (distribution 1); orientations are normalised
+ * N(0, I3) samples (uniform on the sphere).  Deterministic in seed.
+ * Replaces tools/gen.py of the reference. */
+rf_status rf_generate_layout(int32_t M, int32_t distribution, double box, double min_dist,
+                             uint64_t seed, double *positions, double *orientations);
+/* Minimum distance between the centre-lines (segments of half-length 1) of
+ * any two fibers; a geometry diagnostic (the kernels are singular at 0). */
+double rf_min_segment_distance(int32_t M, const double *positions, const double *orientations);
+
+/* ---- Learned preconditioner ----------------------------------------------
+ * MLP: k=16 nearest-neighbour features (relative centre, orientation of the
+ * neighbour, orientation of the fiber: 16 x 9 floats) -> 256 -> 256 -> 225,
+ * ReLU, predicting a correction to the identity preconditioner block.
+ * Weights are FP32, layer-major: W1[256x144] b1[256] W2[256x256] b2[256]
+ * W3[225x256] b3[225] (row-major, out x in). */
+#define RF_MLP_K 16
+#define RF_MLP_IN (RF_MLP_K * 9)
+#define RF_MLP_HIDDEN 256
+#define RF_MLP_OUT 225
+int64_t rf_mlp_num_params(void);
+/* Install weights used by RF_PC_LEARNED. */
+rf_status rf_set_mlp_weights(rf_handle *h, const float *weights, int64_t count);
+/* Features (M x 144) of the current state. */
+rf_status rf_compute_features(rf_handle *h, float *features);
+/* Exact cluster block inverses minus identity (M x 225, row-major 15x15 per
+ * fiber) of the current assembled system: the training targets. */
+rf_status rf_compute_cluster_targets(rf_handle *h, float *targets);
+
+/* Stand-alone trainer on the device: owns weights, Adam state and a dataset. */
+typedef struct rf_trainer rf_trainer;
+rf_status rf_trainer_create(int32_t device, uint64_t seed, rf_trainer **out);
+rf_status rf_trainer_destroy(rf_trainer *t);
+rf_status rf_trainer_add_samples(rf_trainer *t, const float *features, const float *targets,
+                                 int64_t count);
+/* Run epochs of minibatch Adam on the MSE loss; returns the mean loss of the
+ * last epoch. */
+rf_status rf_trainer_train(rf_trainer *t, int32_t epochs, int32_t batch, float lr, float *loss);
+rf_status rf_trainer_get_weights(rf_trainer *t, float *weights);
+rf_status rf_trainer_set_weights(rf_trainer *t, const float *weights);
+/* Forward + backward of one batch with the trainer's weights: loss and
+ * gradient (rf_mlp_num_params floats), for gradient checks. */
+rf_status rf_trainer_loss_grad(rf_trainer *t, const float *features, const float *targets,
+                               int64_t count, float *loss, float *grad);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RIGIDFIBERS_H_ */

@@ -1,0 +1,753 @@
+// api.cu - the C ABI (include/rigidfibers.h): handle life cycle and the
+// reference step API (src/simulation.cu:40-424 of the reference):
+// assemble_system -> solve_system -> update_velocities -> update_fibers.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "handle.h"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * count);
+}
+
+void free_all(rf_handle *h) {
+    for (int i = 0; i < 3; ++i) {
+        cudaFree(h->X[i]);
+        cudaFree(h->T[i]);
+    }
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(h->V[i]);
+        cudaFree(h->W[i]);
+    }
+    void *ptrs[] = {h->tab, h->A64, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
+                    h->PV32, h->PW32, h->vpart, h->pvx, h->pwx, h->work64, h->work32, h->r64, h->r32,
+                    h->d32, h->x32, h->Pblocks, h->knn, h->mlp_w, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out,
+                    h->dscal, h->rb.partials, h->rb.counter};
+    for (void *p : ptrs) cudaFree(p);
+    h->gm64.reset();
+    h->gm32.reset();
+    if (h->hscal) cudaFreeHost(h->hscal);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// Tables of quadrature points, weights, Legendre values and model constants
+// (quadrature.f90:44-84, matrix_assembly.f90:36-56 and 450-484).
+void make_tables(const rf_params &p, rf::Tables &t) {
+    std::memset(&t, 0, sizeof(t));
+    const int NoQI = p.num_quadrature_intervals, N = p.num_terms_in_force_expansion;
+    t.N = N;
+    t.LQ = 3 * NoQI;
+    const double pv0[3] = {-std::sqrt(15.0) / 5.0, 0.0, std::sqrt(15.0) / 5.0};
+    const double wv0[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    double a = -1.0;
+    const double iv = 2.0 / NoQI;
+    for (int i = 0; i < NoQI; ++i) {
+        for (int k = 0; k < 3; ++k) {
+            t.pv[3 * i + k] = (2.0 * a + iv + pv0[k] * iv) / 2.0;
+            t.wv[3 * i + k] = wv0[k] / NoQI;
+        }
+        a = a + iv;
+    }
+    // Legendre polynomials at the points with the explicit formulas of
+    // compute_LVecs (matrix_assembly.f90:36-56); P_0 = 1
+    for (int q = 0; q < t.LQ; ++q) {
+        const double x = t.pv[q];
+        t.P[0][q] = 1.0;
+        for (int m = 1; m <= N; ++m) {
+            double v;
+            switch (m) {
+                case 1: v = x; break;
+                case 2: v = 0.5 * (3.0 * x * x - 1.0); break;
+                case 3: v = 0.5 * (5.0 * x * x * x - 3.0 * x); break;
+                case 4: v = 0.125 * (35.0 * std::pow(x, 4) - 30.0 * x * x + 3.0); break;
+                case 5: v = 0.125 * (63.0 * std::pow(x, 5) - 70.0 * x * x * x + 15.0 * x); break;
+                case 6: v = 0.0625 * (231.0 * std::pow(x, 6) - 315.0 * std::pow(x, 4) + 105.0 * x * x - 5.0); break;
+                case 7:
+                    v = 0.0625 * (429.0 * std::pow(x, 7) - 693.0 * std::pow(x, 5) + 315.0 * x * x * x - 35.0 * x);
+                    break;
+                default:
+                    v = 6435.0 / 128.0 * std::pow(x, 8) - 3003.0 / 32.0 * std::pow(x, 6) + 3465.0 / 64.0 * std::pow(x, 4) -
+                        315.0 / 32.0 * x * x + 35.0 / 128.0;
+                    break;
+            }
+            t.P[m][q] = v;
+        }
+    }
+    const double eps = p.slenderness;
+    const double c = std::log(eps * eps * std::exp(1.0));
+    t.d = -c;
+    t.e = 2.0;
+    t.eps2 = eps * eps;
+    t.D1 = 0.75 / (t.d - 2.0);
+    double lambda[rf::kMaxN + 1] = {0};
+    lambda[1] = 2.0;
+    for (int k = 2; k <= N; ++k) lambda[k] = lambda[k - 1] + 2.0 / k;
+    for (int k = 1; k <= N; ++k) {
+        t.Ek[k] = (t.d - t.e - lambda[k]) / 2.0 / (t.d - lambda[k]);
+        t.gamma[k] = 0.5 * (2.0 * k + 1.0) / (t.d + t.e - lambda[k]);
+    }
+    for (int a2 = 0; a2 < 3; ++a2) {
+        t.force[a2] = p.external_force[a2];
+        t.half_force[a2] = 0.5 * p.external_force[a2];
+    }
+}
+
+bool finite_all(const double *v, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return false;
+    return true;
+}
+
+#define CK(h, expr, what)                                        \
+    do {                                                         \
+        cudaError_t e__ = (expr);                                \
+        if (e__ != cudaSuccess) return rf::cuda_fail(h, e__, what); \
+    } while (0)
+
+bool is_mixed(int prec) { return prec == RF_PREC_MIXED_BF16 || prec == RF_PREC_MIXED_FP32; }
+
+}  // namespace
+
+namespace rf {
+
+rf_status fail(rf_handle *h, rf_status s, const std::string &msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return s;
+}
+
+rf_status cuda_fail(rf_handle *h, cudaError_t e, const char *what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    const rf_status s = (e == cudaErrorMemoryAllocation) ? RF_ERR_OOM
+                        : (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) ? RF_ERR_NO_DEVICE
+                                                                                         : RF_ERR_CUDA;
+    cudaGetLastError();  // clear a sticky launch error
+    return fail(h, s, msg);
+}
+
+}  // namespace rf
+
+extern "C" {
+
+void rf_params_default(rf_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->slenderness = 0.01;
+    p->timestep = 0.1;
+    p->num_fibers = 0;
+    p->num_timesteps = 10;
+    p->num_terms_in_force_expansion = 5;
+    p->num_quadrature_intervals = 8;
+    p->use_analytical_integration = 1;
+    p->use_direct_solver = 0;
+    p->gmres_restart = 10;
+    p->gmres_max_iters = 100;
+    p->gmres_tol = 1e-5;
+    p->external_force[0] = 0.0;
+    p->external_force[1] = 0.0;
+    p->external_force[2] = -1.0;
+    p->precision = RF_PREC_FP64;
+    p->preconditioner = RF_PC_NONE;
+    p->velocity_mode = RF_VEL_RECOMPUTE;
+    p->device = 0;
+    p->max_refinements = 30;
+    p->cluster_size = 12;
+    p->inner_tol = 1e-3;
+    p->near_field_c = 10.0;
+}
+
+const char *rf_status_string(rf_status s) {
+    switch (s) {
+        case RF_OK: return "ok";
+        case RF_ERR_INVALID_ARG: return "invalid argument";
+        case RF_ERR_OOM: return "out of device memory";
+        case RF_ERR_CUDA: return "CUDA error";
+        case RF_ERR_NOT_CONVERGED: return "GMRES did not converge";
+        case RF_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+        case RF_ERR_NAN: return "non-finite value";
+        case RF_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char *rf_last_error(const rf_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+rf_status rf_create(const rf_params *p, const double *positions, const double *orientations, rf_handle **out) {
+    if (!out) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    if (!p || !positions || !orientations) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "null argument");
+    const int M = p->num_fibers, N = p->num_terms_in_force_expansion, NoQI = p->num_quadrature_intervals;
+    if (M < 2) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_fibers must be >= 2");
+    if (N < 1 || N > rf::kMaxN) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_terms_in_force_expansion must be 1..8");
+    if (NoQI < 1 || 3 * NoQI > rf::kMaxLQ)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_quadrature_intervals must be 1..16");
+    if (!(p->slenderness > 0.0 && p->slenderness < 0.5))
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "slenderness must be in (0, 0.5)");
+    if (p->precision < RF_PREC_FP64 || p->precision > RF_PREC_MIXED_FP32)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown precision");
+    if (p->preconditioner < RF_PC_NONE || p->preconditioner > RF_PC_LEARNED)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown preconditioner");
+    if (p->velocity_mode != RF_VEL_RECOMPUTE && p->velocity_mode != RF_VEL_REUSE)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown velocity mode");
+    if (p->use_direct_solver)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "use_direct_solver: the dense LU path is not built; use GMRES");
+    if (p->gmres_restart < 1 || p->gmres_restart > 64 || !(p->gmres_tol > 0.0))
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "gmres_restart must be 1..64 and gmres_tol > 0");
+    if (!finite_all(positions, 3 * (size_t)M) || !finite_all(orientations, 3 * (size_t)M))
+        return rf::fail(nullptr, RF_ERR_NAN, "non-finite position or orientation");
+    for (int i = 0; i < M; ++i) {
+        const double *t = orientations + 3 * i;
+        if (t[0] * t[0] + t[1] * t[1] + t[2] * t[2] < 1e-24)
+            return rf::fail(nullptr, RF_ERR_INVALID_ARG, "zero orientation vector");
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return rf::fail(nullptr, RF_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (p->device < 0 || p->device >= ndev) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "bad device ordinal");
+
+    rf_handle *h = new rf_handle;
+    h->p = *p;
+    h->M = M;
+    h->N = N;
+    h->LQ = 3 * NoQI;
+    h->n = 3LL * N * M;
+    h->lda = round_up(h->n, 64);
+    h->ldp = round_up(3LL * M, 64);
+    h->device = p->device;
+    auto bail = [&](cudaError_t err, const char *what) {
+        rf_status s = rf::cuda_fail(nullptr, err, what);
+        free_all(h);
+        delete h;
+        return s;
+    };
+#define CKC(expr, what)                           \
+    do {                                          \
+        cudaError_t e__ = (expr);                 \
+        if (e__ != cudaSuccess) return bail(e__, what); \
+    } while (0)
+    CKC(cudaSetDevice(h->device), "cudaSetDevice");
+    CKC(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device), "device query");
+    CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+    CKC(cudaEventCreate(&h->ev0), "event");
+    CKC(cudaEventCreate(&h->ev1), "event");
+    const size_t m3 = 3 * (size_t)M;
+    for (int i = 0; i < 3; ++i) {
+        CKC(dalloc(&h->X[i], m3), "alloc state");
+        CKC(dalloc(&h->T[i], m3), "alloc state");
+        CKC(cudaMemset(h->X[i], 0, m3 * 8), "memset");
+        CKC(cudaMemset(h->T[i], 0, m3 * 8), "memset");
+    }
+    for (int i = 0; i < 2; ++i) {
+        CKC(dalloc(&h->V[i], m3), "alloc state");
+        CKC(dalloc(&h->W[i], m3), "alloc state");
+        CKC(cudaMemset(h->V[i], 0, m3 * 8), "memset");
+        CKC(cudaMemset(h->W[i], 0, m3 * 8), "memset");
+    }
+    make_tables(*p, h->tab_h);
+    CKC(dalloc(&h->tab, 1), "alloc tables");
+    CKC(cudaMemcpy(h->tab, &h->tab_h, sizeof(rf::Tables), cudaMemcpyHostToDevice), "upload tables");
+
+    const size_t asz = (size_t)h->lda * (size_t)h->n;
+    const int prec = p->precision;
+    if (prec == RF_PREC_FP64) {
+        CKC(dalloc(&h->A64, asz), "alloc A (FP64)");
+        CKC(cudaMemset(h->A64, 0, asz * 8), "memset A");
+    } else {
+        CKC(dalloc(&h->A32, asz), "alloc A (FP32)");
+        CKC(cudaMemset(h->A32, 0, asz * 4), "memset A");
+        if (prec == RF_PREC_MIXED_BF16) {
+            CKC(dalloc(&h->A16, asz), "alloc A (BF16)");
+            CKC(cudaMemset(h->A16, 0, asz * 2), "memset A");
+        }
+    }
+    // assembly chunking: about 8 CTAs per SM in the grid
+    const int tiles = (M + 7) / 8;
+    int chunks = std::max(1, std::min(M, (h->sm_count * 8 + tiles - 1) / tiles));
+    h->asm_chunk = (M + chunks - 1) / chunks;
+    h->asm_chunks = (M + h->asm_chunk - 1) / h->asm_chunk;
+    h->vel_chunk = h->asm_chunk;
+    h->vel_chunks = h->asm_chunks;
+    CKC(dalloc(&h->b, h->n), "alloc b");
+    CKC(dalloc(&h->x, h->n), "alloc x");
+    CKC(cudaMemset(h->x, 0, h->n * 8), "memset x");
+    CKC(cudaMemset(h->b, 0, h->n * 8), "memset b");
+    CKC(dalloc(&h->bpart, (size_t)h->asm_chunks * h->n), "alloc rhs partials");
+    CKC(dalloc(&h->velpart, (size_t)h->vel_chunks * 6 * M), "alloc velocity partials");
+    if (p->velocity_mode == RF_VEL_REUSE) {
+        const size_t psz = (size_t)h->ldp * (size_t)h->n;
+        if (prec == RF_PREC_FP64) {
+            CKC(dalloc(&h->PV64, psz), "alloc velocity panel");
+            CKC(dalloc(&h->PW64, psz), "alloc velocity panel");
+            CKC(cudaMemset(h->PV64, 0, psz * 8), "memset panel");
+            CKC(cudaMemset(h->PW64, 0, psz * 8), "memset panel");
+        } else {
+            CKC(dalloc(&h->PV32, psz), "alloc velocity panel");
+            CKC(dalloc(&h->PW32, psz), "alloc velocity panel");
+            CKC(cudaMemset(h->PV32, 0, psz * 4), "memset panel");
+            CKC(cudaMemset(h->PW32, 0, psz * 4), "memset panel");
+        }
+        CKC(dalloc(&h->vpart, (size_t)h->asm_chunks * 6 * M), "alloc velocity partials");
+        CKC(dalloc(&h->pvx, m3), "alloc");
+        CKC(dalloc(&h->pwx, m3), "alloc");
+    }
+    // matvec workspace: the largest split buffer over the element sizes in use
+    h->work_elems = std::max({rf::gemv_work_elems(h->lda, h->sm_count, 8), rf::gemv_work_elems(h->lda, h->sm_count, 4),
+                              rf::gemv_work_elems(h->lda, h->sm_count, 2), rf::gemv_work_elems(h->ldp, h->sm_count, 8),
+                              rf::gemv_work_elems(h->ldp, h->sm_count, 4)});
+    CKC(dalloc(&h->work64, h->work_elems), "alloc matvec workspace");
+    CKC(dalloc(&h->work32, h->work_elems), "alloc matvec workspace");
+    CKC(dalloc(&h->dscal, 8), "alloc scalars");
+    CKC(cudaMallocHost(&h->hscal, 8 * sizeof(double)), "alloc pinned scalars");
+    h->rb.max_blocks = 1024;
+    CKC(dalloc(&h->rb.partials, h->rb.max_blocks), "alloc reduction buffer");
+    CKC(dalloc(&h->rb.counter, 1), "alloc reduction counter");
+    CKC(cudaMemset(h->rb.counter, 0, sizeof(unsigned int)), "memset");
+    const int m = p->gmres_restart;
+    if (prec == RF_PREC_FP64) {
+        h->gm64.reset(new rf::Gmres<double>());
+        CKC(h->gm64->init(h->n, m, h->stream), "GMRES workspace");
+    } else {
+        h->gm32.reset(new rf::Gmres<float>());
+        CKC(h->gm32->init(h->n, m, h->stream), "GMRES workspace");
+        CKC(dalloc(&h->r64, h->n), "alloc");
+        CKC(dalloc(&h->r32, h->n), "alloc");
+        CKC(dalloc(&h->d32, h->n), "alloc");
+        CKC(dalloc(&h->x32, h->n), "alloc");
+    }
+#undef CKC
+    h->cur = 1;
+    h->prev = 0;
+    h->next = 2;
+    rf_status s = rf_set_state(h, positions, orientations);
+    if (s != RF_OK) {
+        g_create_error = h->err;
+        free_all(h);
+        delete h;
+        return s;
+    }
+    *out = h;
+    return RF_OK;
+}
+
+rf_status rf_destroy(rf_handle *h) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return RF_OK;
+}
+
+rf_status rf_set_state(rf_handle *h, const double *positions, const double *orientations) {
+    if (!h || !positions || !orientations) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    const size_t m3 = 3 * (size_t)h->M;
+    if (!finite_all(positions, m3) || !finite_all(orientations, m3))
+        return rf::fail(h, RF_ERR_NAN, "non-finite position or orientation");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    CK(h, cudaMemcpyAsync(h->X[h->cur], positions, m3 * 8, cudaMemcpyHostToDevice, h->stream), "upload positions");
+    CK(h, cudaMemcpyAsync(h->T[h->cur], orientations, m3 * 8, cudaMemcpyHostToDevice, h->stream),
+       "upload orientations");
+    // orientations are normalised as in advect_fibers.f90:332-340
+    CK(h, rf::launch_normalize(h->M, h->T[h->cur], h->stream), "normalize");
+    h->launches++;
+    CK(h, cudaStreamSynchronize(h->stream), "sync");
+    h->assembled = false;
+    h->pc_ready = false;
+    return RF_OK;
+}
+
+rf_status rf_assemble_system(rf_handle *h) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    rf::AsmArgs a{};
+    a.M = h->M;
+    a.N = h->N;
+    a.LQ = h->LQ;
+    a.n = h->n;
+    a.pos = h->X[h->cur];
+    a.ori = h->T[h->cur];
+    a.tab = h->tab;
+    a.A64 = h->A64;
+    a.A32 = h->A32;
+    a.A16 = h->A16;
+    a.lda = h->lda;
+    a.bpart = h->bpart;
+    a.PV64 = h->PV64;
+    a.PW64 = h->PW64;
+    a.PV32 = h->PV32;
+    a.PW32 = h->PW32;
+    a.ldp = h->ldp;
+    a.vpart = h->vpart;
+    a.chunk = h->asm_chunk;
+    const int prec = h->p.precision;
+    if (prec == RF_PREC_FP32) {
+        a.near_c = 0.0;        // plain FP32 method: every pair in FP32
+        a.axis_ratio = 0.0;
+    } else {
+        a.near_c = h->p.near_field_c > 0.0 ? h->p.near_field_c : 10.0;
+        a.axis_ratio = 1.0 / 16.0;
+    }
+    const int pmode = prec == RF_PREC_FP64 ? rf::kPModeFP64 : rf::kPModeMixed;
+    CK(h, rf::launch_assemble(a, h->p.use_analytical_integration == 0, pmode, h->asm_chunks, h->stream),
+       "assemble kernel");
+    CK(h, rf::launch_reduce_chunks(h->bpart, h->asm_chunks, h->n, h->n, h->b, h->stream), "rhs reduction");
+    h->launches += 2;
+    if (h->p.preconditioner != RF_PC_NONE) {
+        rf_status s = rf::build_preconditioner(h);
+        if (s != RF_OK) return s;
+    }
+    CK(h, cudaStreamSynchronize(h->stream), "assembly");
+    h->assembled = true;
+    return RF_OK;
+}
+
+rf_status rf_solve_system(rf_handle *h) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    if (!h->assembled) return rf::fail(h, RF_ERR_INVALID_ARG, "solve_system before assemble_system");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const int prec = h->p.precision;
+    const int m = h->p.gmres_restart;
+    const double tol = h->p.gmres_tol;
+    const int maxit = h->p.gmres_max_iters;
+    cudaStream_t st = h->stream;
+    h->stats = rf_solve_stats();
+    CK(h, cudaEventRecord(h->ev0, st), "event");
+    const bool use_pc = h->p.preconditioner != RF_PC_NONE && h->pc_ready;
+    const int nb = 3 * h->N;
+    rf::GmresResult res;
+    rf_status status = RF_OK;
+    if (prec == RF_PREC_FP64) {
+        rf::Gmres<double>::Op A = [h](const double *in, double *out) {
+            h->launches += 2;
+            return rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, in, out, nullptr,
+                                                                   h->work64, h->work_elems, h->sm_count, h->stream);
+        };
+        rf::Gmres<double>::Op P = [h, nb](const double *in, double *out) {
+            return rf::launch_block_apply<double>(h->M, nb, h->Pblocks, in, out, h->stream);
+        };
+        CK(h, h->gm64->solve(A, use_pc ? &P : nullptr, h->b, h->x, false, tol, maxit, &res), "GMRES");
+        if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
+        h->launches += res.launches;
+        h->stats.iterations = res.iterations;
+        h->stats.matvecs = res.matvecs;
+        h->stats.residual = res.backward_error;
+        h->stats.converged = res.info == 0;
+    } else if (prec == RF_PREC_FP32) {
+        rf::Gmres<float>::Op A = [h](const float *in, float *out) {
+            h->launches += 2;
+            return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
+                                                               h->work32, h->work_elems, h->sm_count, h->stream);
+        };
+        rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
+            return rf::launch_block_apply<float>(h->M, nb, h->Pblocks, in, out, h->stream);
+        };
+        CK(h, (rf::launch_convert<float, double>(h->n, h->x, h->x32, st)), "convert");
+        CK(h, (rf::launch_convert<float, double>(h->n, h->b, h->r32, st)), "convert");
+        h->launches += 2;
+        CK(h, h->gm32->solve(A, use_pc ? &P : nullptr, h->r32, h->x32, false, tol, maxit, &res), "GMRES");
+        if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
+        CK(h, (rf::launch_convert<double, float>(h->n, h->x32, h->x, st)), "convert");
+        h->launches += res.launches + 1;
+        h->stats.iterations = res.iterations;
+        h->stats.matvecs = res.matvecs;
+        h->stats.residual = res.backward_error;
+        h->stats.converged = res.info == 0;
+    } else {
+        // Mixed precision: inner GMRES on the low-precision matrix (FP32
+        // vectors and accumulation, FP64 Hessenberg/Givens), outer iterative
+        // refinement with the residual b - A x accumulated in FP64 against
+        // the FP32-stored matrix.
+        const bool bf16 = prec == RF_PREC_MIXED_BF16;
+        rf::Gmres<float>::Op Alo = [h, bf16](const float *in, float *out) {
+            h->launches += 2;
+            if (bf16)
+                return rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, h->n, h->n, in, out,
+                                                                           nullptr, h->work32, h->work_elems,
+                                                                           h->sm_count, h->stream);
+            return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
+                                                               h->work32, h->work_elems, h->sm_count, h->stream);
+        };
+        rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
+            return rf::launch_block_apply<float>(h->M, nb, h->Pblocks, in, out, h->stream);
+        };
+        double *dnorm = h->dscal;
+        const rf::RedBuf &rb = h->rb;
+        auto norm_of = [&](const double *v, double *hv) -> cudaError_t {
+            cudaError_t e = rf::launch_dot<double>(h->n, v, v, dnorm, rb, st);
+            if (e != cudaSuccess) return e;
+            h->launches++;
+            e = cudaMemcpyAsync(h->hscal, dnorm, sizeof(double), cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) return e;
+            e = cudaStreamSynchronize(st);
+            *hv = std::sqrt(h->hscal[0]);
+            return e;
+        };
+        auto residual = [&]() -> cudaError_t {  // r64 = b - A32 x (FP64 accumulation)
+            h->launches += 2;
+            h->stats.matvecs++;
+            return rf::launch_gemv<float, double, double, double>(h->A32, h->lda, h->n, h->n, h->x, h->r64, h->b,
+                                                                  h->work64, h->work_elems, h->sm_count, st);
+        };
+        double bn = 0.0, rn = 0.0;
+        cudaError_t e = norm_of(h->b, &bn);
+        if (e == cudaSuccess) e = residual();
+        if (e == cudaSuccess) e = norm_of(h->r64, &rn);
+        if (e == cudaSuccess && !(std::isfinite(bn) && std::isfinite(rn)))
+            return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
+        int it = 0, iters = 0;
+        const int max_ref = h->p.max_refinements > 0 ? h->p.max_refinements : 30;
+        const double itol = h->p.inner_tol > 0.0 ? h->p.inner_tol : 1e-3;
+        while (e == cudaSuccess && bn > 0.0 && rn / bn > tol && it < max_ref && iters < maxit * max_ref) {
+            // d = argmin |r/rn - A_lo d|, then x += rn * d
+            e = rf::launch_scale_h<float, double>(h->n, h->r64, 1.0 / rn, h->r32, st);
+            if (e != cudaSuccess) break;
+            h->launches++;
+            e = cudaMemsetAsync(h->d32, 0, sizeof(float) * h->n, st);
+            if (e != cudaSuccess) break;
+            e = h->gm32->solve(Alo, use_pc ? &P : nullptr, h->r32, h->d32, true, itol, maxit, &res);
+            if (e != cudaSuccess) break;
+            if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
+            h->launches += res.launches;
+            iters += res.iterations;
+            h->stats.matvecs += res.matvecs;
+            e = rf::launch_axpy_fd(h->n, rn, h->d32, h->x, st);
+            if (e != cudaSuccess) break;
+            h->launches++;
+            e = residual();
+            if (e == cudaSuccess) e = norm_of(h->r64, &rn);
+            ++it;
+        }
+        CK(h, e, "mixed-precision solve");
+        h->stats.iterations = iters;
+        h->stats.refinements = it;
+        h->stats.residual = bn > 0.0 ? rn / bn : 0.0;
+        h->stats.converged = bn == 0.0 || rn / bn <= tol;
+    }
+    CK(h, cudaEventRecord(h->ev1, st), "event");
+    CK(h, cudaEventSynchronize(h->ev1), "event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.seconds = ms * 1e-3;
+    if (!h->stats.converged) status = rf::fail(h, RF_ERR_NOT_CONVERGED, "GMRES budget spent above tolerance");
+    return status;
+}
+
+rf_status rf_update_velocities(rf_handle *h) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    cudaStream_t st = h->stream;
+    double *V = h->V[h->vcur], *W = h->W[h->vcur];
+    if (h->p.velocity_mode == RF_VEL_REUSE) {
+        if (!h->assembled) return rf::fail(h, RF_ERR_INVALID_ARG, "reuse velocities need an assembled system");
+        const int64_t m3 = 3LL * h->M;
+        if (h->PV64) {
+            CK(h, (rf::launch_gemv<double, double, double, double>(h->PV64, h->ldp, m3, h->n, h->x, h->pvx, nullptr,
+                                                                    h->work64, h->work_elems, h->sm_count, st)),
+               "velocity panel");
+            CK(h, (rf::launch_gemv<double, double, double, double>(h->PW64, h->ldp, m3, h->n, h->x, h->pwx, nullptr,
+                                                                    h->work64, h->work_elems, h->sm_count, st)),
+               "velocity panel");
+        } else {
+            CK(h, (rf::launch_gemv<float, double, double, double>(h->PV32, h->ldp, m3, h->n, h->x, h->pvx, nullptr,
+                                                                   h->work64, h->work_elems, h->sm_count, st)),
+               "velocity panel");
+            CK(h, (rf::launch_gemv<float, double, double, double>(h->PW32, h->ldp, m3, h->n, h->x, h->pwx, nullptr,
+                                                                   h->work64, h->work_elems, h->sm_count, st)),
+               "velocity panel");
+        }
+        CK(h, rf::launch_velocity_reuse_finish(h->M, h->T[h->cur], h->tab, h->pvx, h->pwx, h->vpart, h->asm_chunks,
+                                               V, W, st),
+           "velocity finish");
+        h->launches += 5;
+    } else {
+        rf::VelArgs a{};
+        a.M = h->M;
+        a.N = h->N;
+        a.LQ = h->LQ;
+        a.pos = h->X[h->cur];
+        a.ori = h->T[h->cur];
+        a.coeffs = h->x;
+        a.tab = h->tab;
+        a.part = h->velpart;
+        a.chunk = h->vel_chunk;
+        CK(h, rf::launch_velocity(a, h->p.use_analytical_integration == 0, h->vel_chunks, st), "velocity kernel");
+        CK(h, rf::launch_velocity_finish(h->M, h->T[h->cur], h->tab, h->velpart, h->vel_chunks, V, W, st),
+           "velocity finish");
+        h->launches += 2;
+    }
+    CK(h, cudaStreamSynchronize(st), "velocities");
+    h->vlast = h->vcur;
+    return RF_OK;
+}
+
+rf_status rf_update_fibers(rf_handle *h, int first_timestep) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    CK(h, rf::launch_advect(h->M, h->p.timestep, first_timestep != 0, h->X[h->prev], h->X[h->cur], h->T[h->prev],
+                            h->T[h->cur], h->V[h->vcur], h->V[h->vprev], h->W[h->vcur], h->W[h->vprev],
+                            h->X[h->next], h->T[h->next], h->stream),
+       "advect");
+    h->launches++;
+    CK(h, cudaStreamSynchronize(h->stream), "advect");
+    // DoubleSwap of velocities and TripleSwap of state (src/simulation.cu:294-298)
+    std::swap(h->vprev, h->vcur);
+    const int old_prev = h->prev;
+    h->prev = h->cur;
+    h->cur = h->next;
+    h->next = old_prev;
+    h->assembled = false;
+    h->pc_ready = false;
+    return RF_OK;
+}
+
+rf_status rf_step(rf_handle *h, size_t current_timestep) {
+    rf_status s = rf_assemble_system(h);
+    if (s != RF_OK) return s;
+    rf_status solve = rf_solve_system(h);
+    if (solve != RF_OK && solve != RF_ERR_NOT_CONVERGED) return solve;
+    s = rf_update_velocities(h);
+    if (s != RF_OK) return s;
+    s = rf_update_fibers(h, current_timestep == 0);
+    if (s != RF_OK) return s;
+    return solve;
+}
+
+rf_status rf_get_state(rf_handle *h, double *positions, double *orientations) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t m3 = 3 * (size_t)h->M;
+    if (positions)
+        CK(h, cudaMemcpyAsync(positions, h->X[h->cur], m3 * 8, cudaMemcpyDeviceToHost, h->stream), "download");
+    if (orientations)
+        CK(h, cudaMemcpyAsync(orientations, h->T[h->cur], m3 * 8, cudaMemcpyDeviceToHost, h->stream), "download");
+    CK(h, cudaStreamSynchronize(h->stream), "download");
+    return RF_OK;
+}
+
+rf_status rf_get_velocities(rf_handle *h, double *translational, double *rotational) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    if (h->vlast < 0) return rf::fail(h, RF_ERR_INVALID_ARG, "no velocities computed yet");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t m3 = 3 * (size_t)h->M;
+    if (translational)
+        CK(h, cudaMemcpyAsync(translational, h->V[h->vlast], m3 * 8, cudaMemcpyDeviceToHost, h->stream), "download");
+    if (rotational)
+        CK(h, cudaMemcpyAsync(rotational, h->W[h->vlast], m3 * 8, cudaMemcpyDeviceToHost, h->stream), "download");
+    CK(h, cudaStreamSynchronize(h->stream), "download");
+    return RF_OK;
+}
+
+rf_status rf_get_coeffs(rf_handle *h, double *x) {
+    if (!h || !x) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    CK(h, cudaMemcpy(x, h->x, h->n * 8, cudaMemcpyDeviceToHost), "download");
+    return RF_OK;
+}
+
+rf_status rf_get_rhs(rf_handle *h, double *b) {
+    if (!h || !b) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    CK(h, cudaMemcpy(b, h->b, h->n * 8, cudaMemcpyDeviceToHost), "download");
+    return RF_OK;
+}
+
+rf_status rf_get_matrix(rf_handle *h, double *A) {
+    if (!h || !A) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const int64_t n = h->n;
+    double *col = nullptr;
+    CK(h, cudaMalloc(&col, sizeof(double) * h->lda), "alloc");
+    cudaError_t e = cudaSuccess;
+    for (int64_t c = 0; c < n && e == cudaSuccess; ++c) {
+        if (h->A64) {
+            e = cudaMemcpyAsync(A + c * n, h->A64 + c * h->lda, n * 8, cudaMemcpyDeviceToHost, h->stream);
+        } else {
+            e = rf::launch_convert<double, float>(n, h->A32 + c * h->lda, col, h->stream);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(A + c * n, col, n * 8, cudaMemcpyDeviceToHost, h->stream);
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(col);
+    CK(h, e, "download matrix");
+    return RF_OK;
+}
+
+rf_status rf_matvec(rf_handle *h, const double *x, double *y) {
+    if (!h || !x || !y) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    double *dx = nullptr, *dy = nullptr;
+    CK(h, cudaMalloc(&dx, h->n * 8), "alloc");
+    cudaError_t e = cudaMalloc(&dy, h->n * 8);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, x, h->n * 8, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        if (h->A64)
+            e = rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, dx, dy, nullptr, h->work64,
+                                                                h->work_elems, h->sm_count, h->stream);
+        else if (h->A16)
+            e = rf::launch_gemv<__nv_bfloat16, double, double, double>(h->A16, h->lda, h->n, h->n, dx, dy, nullptr,
+                                                                       h->work64, h->work_elems, h->sm_count,
+                                                                       h->stream);
+        else
+            e = rf::launch_gemv<float, double, double, double>(h->A32, h->lda, h->n, h->n, dx, dy, nullptr, h->work64,
+                                                               h->work_elems, h->sm_count, h->stream);
+        h->launches += 2;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy, h->n * 8, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dx);
+    cudaFree(dy);
+    CK(h, e, "matvec");
+    return RF_OK;
+}
+
+rf_status rf_get_solve_stats(rf_handle *h, rf_solve_stats *s) {
+    if (!h || !s) return RF_ERR_INVALID_ARG;
+    *s = h->stats;
+    return RF_OK;
+}
+
+rf_status rf_get_history(rf_handle *h, double *prev_pos, double *prev_orient, double *prev_vel, double *prev_rot) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t m3 = 3 * (size_t)h->M * 8;
+    if (prev_pos) CK(h, cudaMemcpy(prev_pos, h->X[h->prev], m3, cudaMemcpyDeviceToHost), "download");
+    if (prev_orient) CK(h, cudaMemcpy(prev_orient, h->T[h->prev], m3, cudaMemcpyDeviceToHost), "download");
+    if (prev_vel) CK(h, cudaMemcpy(prev_vel, h->V[h->vprev], m3, cudaMemcpyDeviceToHost), "download");
+    if (prev_rot) CK(h, cudaMemcpy(prev_rot, h->W[h->vprev], m3, cudaMemcpyDeviceToHost), "download");
+    return RF_OK;
+}
+
+rf_status rf_set_history(rf_handle *h, const double *prev_pos, const double *prev_orient, const double *prev_vel,
+                         const double *prev_rot, const double *coeffs) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const size_t m3 = 3 * (size_t)h->M * 8;
+    if (prev_pos) CK(h, cudaMemcpy(h->X[h->prev], prev_pos, m3, cudaMemcpyHostToDevice), "upload");
+    if (prev_orient) CK(h, cudaMemcpy(h->T[h->prev], prev_orient, m3, cudaMemcpyHostToDevice), "upload");
+    if (prev_vel) CK(h, cudaMemcpy(h->V[h->vprev], prev_vel, m3, cudaMemcpyHostToDevice), "upload");
+    if (prev_rot) CK(h, cudaMemcpy(h->W[h->vprev], prev_rot, m3, cudaMemcpyHostToDevice), "upload");
+    if (coeffs) CK(h, cudaMemcpy(h->x, coeffs, h->n * 8, cudaMemcpyHostToDevice), "upload");
+    return RF_OK;
+}
+
+int64_t rf_system_size(const rf_handle *h) { return h ? h->n : 0; }
+int64_t rf_matrix_ld(const rf_handle *h) { return h ? h->lda : 0; }
+void *rf_get_stream(rf_handle *h) { return h ? (void *)h->stream : nullptr; }
+int64_t rf_kernel_launches(const rf_handle *h) { return h ? h->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+// handle.h - the rf_handle behind the C ABI (internal).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+
+#include "../../include/rigidfibers.h"
+#include "gmres.h"
+#include "rf_kernels.h"
+
+struct rf_handle {
+    rf_params p{};
+    int M = 0, N = 0, LQ = 0;
+    int64_t n = 0;        // 3*N*M
+    int64_t lda = 0;      // leading dimension of A (multiple of 64 elements)
+    int64_t ldp = 0;      // leading dimension of the velocity panels
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    // state: positions/orientations triple-buffered, velocities double-buffered
+    double *X[3] = {nullptr, nullptr, nullptr};
+    double *T[3] = {nullptr, nullptr, nullptr};
+    int prev = 0, cur = 1, next = 2;
+    double *V[2] = {nullptr, nullptr};
+    double *W[2] = {nullptr, nullptr};
+    int vprev = 0, vcur = 1;
+    int vlast = -1;           // slot of the most recent velocities
+
+    // system
+    rf::Tables tab_h{};
+    rf::Tables *tab = nullptr;
+    double *A64 = nullptr;
+    float *A32 = nullptr;
+    __nv_bfloat16 *A16 = nullptr;
+    double *b = nullptr;       // right-hand side
+    double *x = nullptr;       // coefficients (warm start for the next solve)
+    double *bpart = nullptr;   // [nchunks][n]
+    int asm_chunks = 1, asm_chunk = 1;
+    int vel_chunks = 1, vel_chunk = 1;
+    double *velpart = nullptr; // [vel_chunks][6M]
+    // velocity panels (reuse mode)
+    double *PV64 = nullptr, *PW64 = nullptr;
+    float *PV32 = nullptr, *PW32 = nullptr;
+    double *vpart = nullptr;   // [asm_chunks][6M]
+    double *pvx = nullptr, *pwx = nullptr;
+    // matvec workspace
+    double *work64 = nullptr;
+    float *work32 = nullptr;
+    int64_t work_elems = 0;
+    // solver
+    std::unique_ptr<rf::Gmres<double>> gm64;
+    std::unique_ptr<rf::Gmres<float>> gm32;
+    double *r64 = nullptr;     // refinement residual
+    float *r32 = nullptr;      // scaled residual / rhs in FP32
+    float *d32 = nullptr;      // inner correction
+    float *x32 = nullptr;      // FP32 iterate (FP32 variant)
+    double *dscal = nullptr;   // device scalars (norms)
+    double *hscal = nullptr;   // pinned host mirror
+    rf::RedBuf rb{};
+    // preconditioner
+    float *Pblocks = nullptr;  // M x (3N)^2 row-major blocks
+    bool pc_ready = false;
+    int *knn = nullptr;        // M x kmax neighbour lists
+    float *mlp_w = nullptr;    // MLP weights on the device
+    bool mlp_loaded = false;
+    float *feat = nullptr;     // M x 144 features
+    float *mlp_h1 = nullptr, *mlp_h2 = nullptr, *mlp_out = nullptr;
+
+    rf_solve_stats stats{};
+    bool assembled = false;
+    int64_t launches = 0;
+    std::string err;
+};
+
+namespace rf {
+rf_status fail(rf_handle *h, rf_status s, const std::string &msg);
+rf_status cuda_fail(rf_handle *h, cudaError_t e, const char *what);
+// preconditioner (precond.cu)
+rf_status build_preconditioner(rf_handle *h);
+rf_status apply_mlp(rf_handle *h);
+}  // namespace rf

@@ -1,0 +1,460 @@
+// linalg.cu - K2 streaming matrix-vector product and K5 Krylov-vector kernels.
+//
+// Reference: the GMRES of lib/viennacl/linalg/gmres.hpp:168-339 with
+// vec_mul_col_kernel (matrix_operations_col.hpp:1251-1278, launched
+// <<<128,128>>>) and the inner_prod/norm kernels of vector_operations.hpp;
+// the Fortran path uses dgemv (coeffs_and_vels.f90:483,492).
+//
+// GEMV.  A is column-major.  A CTA of 256 threads owns a tile of 256*VEC
+// consecutive rows (VEC = 16 bytes / element size) and a contiguous range of
+// columns; every column contributes one 16-byte streaming load per thread
+// (fully coalesced 4 KB per CTA and column).  Column ranges split the matrix
+// so that the grid fills every SM several times; per-split partial sums are
+// added in a fixed order by a second kernel (deterministic, no atomics).
+//
+// Reductions.  Dot products and norms use one pass with a per-block partial,
+// and the last block to finish (ticket counter, no spinning) adds the
+// partials in block order and writes the scalar to device memory.
+#include "rf_kernels.h"
+
+namespace rf {
+
+namespace {
+
+template <typename S>
+struct Vec16;
+template <>
+struct Vec16<double> {
+    static constexpr int kVec = 2;
+    template <typename ACC>
+    __device__ __forceinline__ static void load(const double *p, ACC *v) {
+        const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+        v[0] = (ACC)t.x;
+        v[1] = (ACC)t.y;
+    }
+};
+template <>
+struct Vec16<float> {
+    static constexpr int kVec = 4;
+    template <typename ACC>
+    __device__ __forceinline__ static void load(const float *p, ACC *v) {
+        const float4 t = __ldcs(reinterpret_cast<const float4 *>(p));
+        v[0] = (ACC)t.x;
+        v[1] = (ACC)t.y;
+        v[2] = (ACC)t.z;
+        v[3] = (ACC)t.w;
+    }
+};
+template <>
+struct Vec16<__nv_bfloat16> {
+    static constexpr int kVec = 8;
+    template <typename ACC>
+    __device__ __forceinline__ static void load(const __nv_bfloat16 *p, ACC *v) {
+        const uint4 t = __ldcs(reinterpret_cast<const uint4 *>(p));
+        const uint32_t w[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            // bf16 -> fp32 is a 16-bit shift
+            v[2 * k] = (ACC)__uint_as_float(w[k] << 16);
+            v[2 * k + 1] = (ACC)__uint_as_float(w[k] & 0xffff0000u);
+        }
+    }
+};
+
+constexpr int kGemvThreads = 256;
+constexpr int kGemvUnroll = 8;
+
+template <typename S, typename X, typename ACC>
+__global__ void __launch_bounds__(kGemvThreads) gemv_partial_kernel(const S *__restrict__ A, int64_t lda, int64_t m,
+                                                                    int64_t k, const X *__restrict__ x,
+                                                                    int64_t cols_per_split, ACC *__restrict__ work,
+                                                                    int64_t mpad) {
+    constexpr int VEC = Vec16<S>::kVec;
+    const int64_t row = ((int64_t)blockIdx.x * kGemvThreads + threadIdx.x) * VEC;
+    const int64_t c0 = (int64_t)blockIdx.y * cols_per_split;
+    const int64_t c1 = min(k, c0 + cols_per_split);
+    ACC acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; ++v) acc[v] = (ACC)0;
+    if (row < lda) {
+        const S *p = A + c0 * lda + row;
+        int64_t c = c0;
+        for (; c + kGemvUnroll <= c1; c += kGemvUnroll) {
+            ACC a[kGemvUnroll][VEC];
+            ACC xv[kGemvUnroll];
+#pragma unroll
+            for (int u = 0; u < kGemvUnroll; ++u) {
+                Vec16<S>::load(p + (int64_t)u * lda, a[u]);
+                xv[u] = (ACC)__ldg(x + c + u);
+            }
+#pragma unroll
+            for (int u = 0; u < kGemvUnroll; ++u)
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) acc[v] += a[u][v] * xv[u];
+            p += (int64_t)kGemvUnroll * lda;
+        }
+        for (; c < c1; ++c) {
+            ACC a[VEC];
+            Vec16<S>::load(p, a);
+            const ACC xv = (ACC)__ldg(x + c);
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) acc[v] += a[v] * xv;
+            p += lda;
+        }
+        ACC *w = work + (int64_t)blockIdx.y * mpad + row;
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) w[v] = acc[v];
+    }
+    (void)m;
+}
+
+template <typename ACC, typename Y>
+__global__ void gemv_reduce_kernel(const ACC *__restrict__ work, int splits, int64_t mpad, int64_t m, Y *y,
+                                   const Y *r) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    ACC s = (ACC)0;
+    for (int t = 0; t < splits; ++t) s += work[(int64_t)t * mpad + i];
+    if (r) y[i] = (Y)((ACC)r[i] - s);
+    else y[i] = (Y)s;
+}
+
+int gemv_splits(int64_t m, int64_t k, int vec, int sm_count) {
+    const int64_t tiles = (m + (int64_t)kGemvThreads * vec - 1) / ((int64_t)kGemvThreads * vec);
+    const int64_t target = (int64_t)sm_count * 8;
+    int64_t splits = (target + tiles - 1) / tiles;
+    const int64_t max_by_cols = k / 256 > 0 ? k / 256 : 1;
+    if (splits > max_by_cols) splits = max_by_cols;
+    if (splits < 1) splits = 1;
+    return (int)splits;
+}
+
+}  // namespace
+
+int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes) {
+    const int vec = 16 / elem_bytes;
+    const int64_t tiles = (m + (int64_t)kGemvThreads * vec - 1) / ((int64_t)kGemvThreads * vec);
+    const int64_t mpad = tiles * kGemvThreads * vec;
+    return (int64_t)gemv_splits(m, m, vec, sm_count) * mpad;
+}
+
+template <typename S, typename X, typename ACC, typename Y>
+cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *x, Y *y, const Y *r, ACC *work,
+                        int64_t work_elems, int sm_count, cudaStream_t st) {
+    constexpr int VEC = Vec16<S>::kVec;
+    const int64_t tiles = (lda + (int64_t)kGemvThreads * VEC - 1) / ((int64_t)kGemvThreads * VEC);
+    const int64_t mpad = tiles * kGemvThreads * VEC;
+    int splits = gemv_splits(m, k, VEC, sm_count);
+    while (splits > 1 && (int64_t)splits * mpad > work_elems) --splits;
+    if ((int64_t)splits * mpad > work_elems) return cudaErrorInvalidValue;
+    const int64_t cps = (k + splits - 1) / splits;
+    dim3 grid((unsigned)tiles, (unsigned)splits);
+    gemv_partial_kernel<S, X, ACC><<<grid, kGemvThreads, 0, st>>>(A, lda, m, k, x, cps, work, mpad);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    gemv_reduce_kernel<ACC, Y><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(work, splits, mpad, m, y, r);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_gemv<double, double, double, double>(const double *, int64_t, int64_t, int64_t,
+                                                                 const double *, double *, const double *,
+                                                                 double *, int64_t, int, cudaStream_t);
+template cudaError_t launch_gemv<float, double, double, double>(const float *, int64_t, int64_t, int64_t,
+                                                                const double *, double *, const double *,
+                                                                double *, int64_t, int, cudaStream_t);
+template cudaError_t launch_gemv<float, float, float, float>(const float *, int64_t, int64_t, int64_t,
+                                                             const float *, float *, const float *, float *,
+                                                             int64_t, int, cudaStream_t);
+template cudaError_t launch_gemv<__nv_bfloat16, float, float, float>(const __nv_bfloat16 *, int64_t, int64_t,
+                                                                     int64_t, const float *, float *,
+                                                                     const float *, float *, int64_t, int,
+                                                                     cudaStream_t);
+template cudaError_t launch_gemv<__nv_bfloat16, double, double, double>(const __nv_bfloat16 *, int64_t, int64_t,
+                                                                        int64_t, const double *, double *,
+                                                                        const double *, double *, int64_t, int,
+                                                                        cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// reductions
+
+namespace {
+
+constexpr int kRedThreads = 256;
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w];
+    }
+    return s;  // valid in thread 0
+}
+
+// The last block to finish adds all block partials in order.
+__device__ __forceinline__ void finish_reduction(double blocksum, const RedBuf &rb, double *out, bool take_sqrt) {
+    __shared__ bool is_last;
+    if (threadIdx.x == 0) {
+        rb.partials[blockIdx.x] = blocksum;
+        __threadfence();
+        const unsigned int ticket = atomicAdd(rb.counter, 1u);
+        is_last = (ticket == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0) {
+        __threadfence();
+        double s = 0.0;
+        for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(rb.partials + b);
+        *out = take_sqrt ? sqrt(s) : s;
+        *rb.counter = 0u;
+    }
+}
+
+inline int red_blocks(int64_t n, const RedBuf &rb) {
+    int64_t b = (n + kRedThreads * 4 - 1) / (kRedThreads * 4);
+    if (b > rb.max_blocks) b = rb.max_blocks;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) mgs_step_kernel(int64_t n, T *w, const T *vprev,
+                                                               const double *hprev, const T *v, double *out,
+                                                               RedBuf rb) {
+    __shared__ double sh[kRedThreads / 32];
+    const double h = vprev ? *hprev : 0.0;
+    double acc = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        T we = w[e];
+        if (vprev) {
+            we = (T)((double)we + (-h) * (double)vprev[e]);
+            w[e] = we;
+        }
+        acc += (double)v[e] * (double)we;
+    }
+    const double s = block_sum(acc, sh);
+    finish_reduction(s, rb, out, false);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) mgs_norm_kernel(int64_t n, T *w, const T *vprev,
+                                                               const double *hprev, double *out, RedBuf rb) {
+    __shared__ double sh[kRedThreads / 32];
+    const double h = vprev ? *hprev : 0.0;
+    double acc = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        T we = w[e];
+        if (vprev) {
+            we = (T)((double)we + (-h) * (double)vprev[e]);
+            w[e] = we;
+        }
+        acc += (double)we * (double)we;
+    }
+    const double s = block_sum(acc, sh);
+    finish_reduction(s, rb, out, true);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) dot_kernel(int64_t n, const T *a, const T *b, double *out,
+                                                          RedBuf rb) {
+    __shared__ double sh[kRedThreads / 32];
+    double acc = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        acc += (double)a[e] * (double)b[e];
+    const double s = block_sum(acc, sh);
+    finish_reduction(s, rb, out, false);
+}
+
+template <typename TO, typename TI>
+__global__ void scale_kernel(int64_t n, const TI *x, const double *den, double num, TO *y) {
+    const double f = num / *den;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] = (TO)(f * (double)x[e]);
+}
+
+template <typename TO, typename TI>
+__global__ void scale_h_kernel(int64_t n, const TI *x, double alpha, TO *y) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] = (TO)(alpha * (double)x[e]);
+}
+
+template <typename TV>
+__global__ void combine_kernel(int64_t n, const double *x, const TV *V, int64_t ldv, const double *y, int k,
+                               double *xcur) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < k; ++c) s += (double)V[(int64_t)c * ldv + e] * y[c];
+        xcur[e] = (x ? x[e] : 0.0) + s;
+    }
+}
+
+template <typename T>
+__global__ void bmr_kernel(int64_t n, const T *b, T *r) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        r[e] = b[e] - r[e];
+}
+
+template <typename T>
+__global__ void vy_kernel(int64_t n, const T *V, int64_t ldv, const double *y, int k, T *u) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int c = 0; c < k; ++c) s += (double)V[(int64_t)c * ldv + e] * y[c];
+        u[e] = (T)s;
+    }
+}
+
+template <typename T>
+__global__ void add_kernel(int64_t n, const T *x, const T *u, T *out) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = x[e] + u[e];
+}
+
+__global__ void axpy_d_kernel(int64_t n, double alpha, const double *x, double *y) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] += alpha * x[e];
+}
+
+__global__ void axpy_fd_kernel(int64_t n, double alpha, const float *d, double *x) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        x[e] += alpha * (double)d[e];
+}
+
+template <typename TO, typename TI>
+__global__ void convert_kernel(int64_t n, const TI *x, TO *y) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        y[e] = (TO)x[e];
+}
+
+template <typename T>
+__global__ void block_apply_kernel(int M, int nb, const float *B, const T *v, T *z) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)M * nb) return;
+    const int64_t i = idx / nb;
+    const int r = (int)(idx - i * nb);
+    const float *b = B + (i * nb + r) * nb;
+    const T *vi = v + i * nb;
+    double s = 0.0;
+    for (int c = 0; c < nb; ++c) s += (double)b[c] * (double)vi[c];
+    z[idx] = (T)s;
+}
+
+inline unsigned grid_for(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    if (b > 4096) b = 4096;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_mgs_step(int64_t n, T *w, const T *vprev, const double *hprev, const T *v, double *out,
+                            const RedBuf &rb, cudaStream_t st) {
+    mgs_step_kernel<T><<<red_blocks(n, rb), kRedThreads, 0, st>>>(n, w, vprev, hprev, v, out, rb);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_mgs_norm(int64_t n, T *w, const T *vprev, const double *hprev, double *out, const RedBuf &rb,
+                            cudaStream_t st) {
+    mgs_norm_kernel<T><<<red_blocks(n, rb), kRedThreads, 0, st>>>(n, w, vprev, hprev, out, rb);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_dot(int64_t n, const T *a, const T *b, double *out, const RedBuf &rb, cudaStream_t st) {
+    dot_kernel<T><<<red_blocks(n, rb), kRedThreads, 0, st>>>(n, a, b, out, rb);
+    return cudaGetLastError();
+}
+template <typename TO, typename TI>
+cudaError_t launch_scale(int64_t n, const TI *x, const double *den, double num, TO *y, cudaStream_t st) {
+    scale_kernel<TO, TI><<<grid_for(n), 256, 0, st>>>(n, x, den, num, y);
+    return cudaGetLastError();
+}
+template <typename TO, typename TI>
+cudaError_t launch_scale_h(int64_t n, const TI *x, double alpha, TO *y, cudaStream_t st) {
+    scale_h_kernel<TO, TI><<<grid_for(n), 256, 0, st>>>(n, x, alpha, y);
+    return cudaGetLastError();
+}
+template cudaError_t launch_scale_h<float, double>(int64_t, const double *, double, float *, cudaStream_t);
+template cudaError_t launch_scale_h<double, double>(int64_t, const double *, double, double *, cudaStream_t);
+
+template <typename TV>
+cudaError_t launch_combine(int64_t n, const double *x, const TV *V, int64_t ldv, const double *y, int k,
+                           double *xcur, cudaStream_t st) {
+    combine_kernel<TV><<<grid_for(n), 256, 0, st>>>(n, x, V, ldv, y, k, xcur);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_bmr(int64_t n, const T *b, T *r, cudaStream_t st) {
+    bmr_kernel<T><<<grid_for(n), 256, 0, st>>>(n, b, r);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_vy(int64_t n, const T *V, int64_t ldv, const double *y, int k, T *u, cudaStream_t st) {
+    vy_kernel<T><<<grid_for(n), 256, 0, st>>>(n, V, ldv, y, k, u);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_add(int64_t n, const T *x, const T *u, T *out, cudaStream_t st) {
+    add_kernel<T><<<grid_for(n), 256, 0, st>>>(n, x, u, out);
+    return cudaGetLastError();
+}
+template cudaError_t launch_bmr<double>(int64_t, const double *, double *, cudaStream_t);
+template cudaError_t launch_bmr<float>(int64_t, const float *, float *, cudaStream_t);
+template cudaError_t launch_vy<double>(int64_t, const double *, int64_t, const double *, int, double *, cudaStream_t);
+template cudaError_t launch_vy<float>(int64_t, const float *, int64_t, const double *, int, float *, cudaStream_t);
+template cudaError_t launch_add<double>(int64_t, const double *, const double *, double *, cudaStream_t);
+template cudaError_t launch_add<float>(int64_t, const float *, const float *, float *, cudaStream_t);
+
+cudaError_t launch_axpy_d(int64_t n, double alpha, const double *x, double *y, cudaStream_t st) {
+    axpy_d_kernel<<<grid_for(n), 256, 0, st>>>(n, alpha, x, y);
+    return cudaGetLastError();
+}
+cudaError_t launch_axpy_fd(int64_t n, double alpha, const float *d, double *x, cudaStream_t st) {
+    axpy_fd_kernel<<<grid_for(n), 256, 0, st>>>(n, alpha, d, x);
+    return cudaGetLastError();
+}
+template <typename TO, typename TI>
+cudaError_t launch_convert(int64_t n, const TI *x, TO *y, cudaStream_t st) {
+    convert_kernel<TO, TI><<<grid_for(n), 256, 0, st>>>(n, x, y);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_block_apply(int M, int nb, const float *B, const T *v, T *z, cudaStream_t st) {
+    const int64_t tot = (int64_t)M * nb;
+    block_apply_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(M, nb, B, v, z);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_mgs_step<double>(int64_t, double *, const double *, const double *, const double *,
+                                             double *, const RedBuf &, cudaStream_t);
+template cudaError_t launch_mgs_step<float>(int64_t, float *, const float *, const double *, const float *,
+                                            double *, const RedBuf &, cudaStream_t);
+template cudaError_t launch_mgs_norm<double>(int64_t, double *, const double *, const double *, double *,
+                                             const RedBuf &, cudaStream_t);
+template cudaError_t launch_mgs_norm<float>(int64_t, float *, const float *, const double *, double *,
+                                            const RedBuf &, cudaStream_t);
+template cudaError_t launch_dot<double>(int64_t, const double *, const double *, double *, const RedBuf &,
+                                        cudaStream_t);
+template cudaError_t launch_dot<float>(int64_t, const float *, const float *, double *, const RedBuf &,
+                                       cudaStream_t);
+template cudaError_t launch_scale<double, double>(int64_t, const double *, const double *, double, double *,
+                                                  cudaStream_t);
+template cudaError_t launch_scale<float, float>(int64_t, const float *, const double *, double, float *,
+                                                cudaStream_t);
+template cudaError_t launch_scale<float, double>(int64_t, const double *, const double *, double, float *,
+                                                 cudaStream_t);
+template cudaError_t launch_combine<double>(int64_t, const double *, const double *, int64_t, const double *,
+                                            int, double *, cudaStream_t);
+template cudaError_t launch_combine<float>(int64_t, const double *, const float *, int64_t, const double *, int,
+                                           double *, cudaStream_t);
+template cudaError_t launch_convert<float, double>(int64_t, const double *, float *, cudaStream_t);
+template cudaError_t launch_convert<double, float>(int64_t, const float *, double *, cudaStream_t);
+template cudaError_t launch_convert<double, __nv_bfloat16>(int64_t, const __nv_bfloat16 *, double *,
+                                                           cudaStream_t);
+template cudaError_t launch_block_apply<double>(int, int, const float *, const double *, double *, cudaStream_t);
+template cudaError_t launch_block_apply<float>(int, int, const float *, const float *, float *, cudaStream_t);
+
+}  // namespace rf

@@ -1,0 +1,123 @@
+// rf_kernels.h - kernel argument blocks and launchers (device side of the
+// library).  Host code in api.cpp and gmres.cpp calls only these launchers.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "rf_device.cuh"
+
+namespace rf {
+
+constexpr int kPModeFP64 = 0;   // FP64 arithmetic throughout
+constexpr int kPModeMixed = 1;  // FP32 far field, FP64 near field, FP32 projections
+
+struct AsmArgs {
+    int M, N, LQ;
+    int64_t n;                 // 3*N*M
+    const double *pos, *ori;   // 3M each
+    const Tables *tab;         // device tables
+    double *A64;               // FP64 matrix or null
+    float *A32;                // FP32 matrix or null
+    __nv_bfloat16 *A16;        // BF16 matrix or null
+    int64_t lda;
+    double *bpart;             // [nchunks][n] partial right-hand sides
+    double *PV64, *PW64;       // velocity panels (3M x n, ld ldp) or null
+    float *PV32, *PW32;
+    int64_t ldp;
+    double *vpart;             // [nchunks][6M] l = 0 velocity terms (or null)
+    int chunk;                 // sources per CTA
+    double near_c;             // mixed: c below which the integral stays FP64
+    double axis_ratio;         // mixed: d < c*axis_ratio stays FP64
+};
+
+cudaError_t launch_assemble(const AsmArgs &a, bool numeric, int pmode, int nchunks, cudaStream_t st);
+cudaError_t launch_reduce_chunks(const double *part, int nchunks, int64_t stride, int64_t len, double *out,
+                                 cudaStream_t st);
+
+// ---- velocities (recompute path) -------------------------------------------
+struct VelArgs {
+    int M, N, LQ;
+    const double *pos, *ori;
+    const double *coeffs;      // n
+    const Tables *tab;
+    double *part;              // [nchunks][6M]: IF0 (3) and IF1 (3) sums per target
+    int chunk;
+};
+cudaError_t launch_velocity(const VelArgs &a, bool numeric, int nchunks, cudaStream_t st);
+// V = (local + 0.5*sum IF0)/d, W = 1.5/d (sum IF1 - (t.sum IF1) t)
+cudaError_t launch_velocity_finish(int M, const double *ori, const Tables *tab, const double *part,
+                                   int nchunks, double *V, double *W, cudaStream_t st);
+// reuse path: V = PV x + v0, W = PW x + w0 (+ local term)
+cudaError_t launch_velocity_reuse_finish(int M, const double *ori, const Tables *tab, const double *pv_x,
+                                         const double *pw_x, const double *vpart, int nchunks, double *V,
+                                         double *W, cudaStream_t st);
+
+// ---- advection ---------------------------------------------------------------
+cudaError_t launch_advect(int M, double dt, bool first, const double *Xp, const double *Xc, const double *Tp,
+                          const double *Tc, const double *Vn, const double *Vo, const double *Wn,
+                          const double *Wo, double *Xn, double *Tn, cudaStream_t st);
+cudaError_t launch_normalize(int M, double *T, cudaStream_t st);
+
+// ---- dense matrix-vector products -------------------------------------------
+// y[0:m) = A[0:m, 0:k) x, A column-major with leading dimension lda.
+// S storage type, X vector type, ACC accumulation type, Y output type.
+// mode 0: y = A x;  mode 1: y = r - A x (residual, r given)
+template <typename S, typename X, typename ACC, typename Y>
+cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *x, Y *y, const Y *r,
+                        ACC *work, int64_t work_elems, int sm_count, cudaStream_t st);
+int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes);
+
+// ---- Krylov vector kernels ----------------------------------------------------
+struct RedBuf {                 // deterministic last-block reduction workspace
+    double *partials;           // >= max blocks
+    unsigned int *counter;      // zero-initialised
+    int max_blocks;
+};
+// w -= hprev * vprev (if vprev); out = dot(v, w)   (modified Gram-Schmidt step)
+template <typename T>
+cudaError_t launch_mgs_step(int64_t n, T *w, const T *vprev, const double *hprev, const T *v, double *out,
+                            const RedBuf &rb, cudaStream_t st);
+// w -= hprev * vprev; out = sqrt(dot(w, w))
+template <typename T>
+cudaError_t launch_mgs_norm(int64_t n, T *w, const T *vprev, const double *hprev, double *out,
+                            const RedBuf &rb, cudaStream_t st);
+// out = dot(a, b) (double accumulation)
+template <typename T>
+cudaError_t launch_dot(int64_t n, const T *a, const T *b, double *out, const RedBuf &rb, cudaStream_t st);
+// y = alpha_scale * x where alpha_scale = num/den (den device scalar), i.e. y = x * (num / *den)
+template <typename TO, typename TI>
+cudaError_t launch_scale(int64_t n, const TI *x, const double *den, double num, TO *y, cudaStream_t st);
+// y = alpha * x (alpha host scalar)
+template <typename TO, typename TI>
+cudaError_t launch_scale_h(int64_t n, const TI *x, double alpha, TO *y, cudaStream_t st);
+// xcur = x + V(:, 0:k) y   (V column-major ld n, y device array of k doubles)
+template <typename TV>
+cudaError_t launch_combine(int64_t n, const double *x, const TV *V, int64_t ldv, const double *y, int k,
+                           double *xcur, cudaStream_t st);
+// r = b - r
+template <typename T>
+cudaError_t launch_bmr(int64_t n, const T *b, T *r, cudaStream_t st);
+// u = V(:, 0:k) y  (y device array of k doubles)
+template <typename T>
+cudaError_t launch_vy(int64_t n, const T *V, int64_t ldv, const double *y, int k, T *u, cudaStream_t st);
+// out = x + u
+template <typename T>
+cudaError_t launch_add(int64_t n, const T *x, const T *u, T *out, cudaStream_t st);
+// y += alpha * x (alpha host scalar)
+cudaError_t launch_axpy_d(int64_t n, double alpha, const double *x, double *y, cudaStream_t st);
+// x += scale * d  with d float, scale host
+cudaError_t launch_axpy_fd(int64_t n, double alpha, const float *d, double *x, cudaStream_t st);
+// convert
+template <typename TO, typename TI>
+cudaError_t launch_convert(int64_t n, const TI *x, TO *y, cudaStream_t st);
+
+// ---- block-diagonal preconditioner (15x15 blocks per fiber, FP32) -------------
+// z = blockdiag(B) v, B[i] row-major 3N x 3N
+template <typename T>
+cudaError_t launch_block_apply(int M, int nb, const float *B, const T *v, T *z, cudaStream_t st);
+
+}  // namespace rf
