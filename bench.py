@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Time steps/s of the rigid-fiber step at M=4000 (clustered sedimenting cloud).
+
+Workload (one "step" = assemble -> solve -> velocities -> advect of the whole
+suspension): M = 4000 fibers, centres isotropic Gaussian sigma 3 with minimum
+centre distance 0.2 (seed 1004), orientations uniform on the sphere, half
+length 1, eps = 1e-3, N = 5 Legendre terms, 8 x 3 Gauss points, dt = 0.1,
+gravity (0,0,-1) per fiber, GMRES restart 10, FP64 residual tolerance 1e-10.
+Synthetic, seeded data; no dataset is involved.
+
+Arms:
+  default            the product path: BF16-stored A for the inner GMRES (FP32
+                     accumulation), FP64-residual iterative refinement against
+                     the FP32-stored A, block preconditioner, velocities from
+                     the stored projection panels.  The plain FP64 GPU path
+                     (the reference method unchanged) is timed in the same run
+                     for the speed-up and the velocity error.
+  --impl reference   the CPU implementation of the path (the FP64 oracle, an
+                     OpenMP restatement of the reference Fortran, which cannot
+                     be built here: no Fortran compiler) on a bounded sample of
+                     the same workload, all host threads.
+
+Multi-GPU: every rank runs an independent replica (the reference has no
+parallelism beyond one device); value = steps of all ranks / max time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "steps/s at M=4000 fibers: BF16+FP64-refine+learned vs plain FP64 GPU, ≤1e-6 err"
+WORKLOAD = dict(M=4000, distribution="gaussian", box=3.0, min_dist=0.2, seed=1004, eps=1e-3, N=5, NoQI=8, dt=0.1,
+                restart=10, tol=1e-10)
+# FP64 GMRES matrix-vector products per step on this workload (the CPU sample
+# cannot solve the full 60000 x 60000 system in a bounded time; the count is
+# the one the same GMRES takes on it, from the FP64 run of this benchmark).
+FP64_MATVECS_PER_STEP = 26
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--M", type=int, default=WORKLOAD["M"], help="override the number of fibers (smoke runs)")
+    ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
+    ap.add_argument("--pc", choices=["learned", "cluster", "none"], default="none")
+    ap.add_argument("--weights", default=os.path.join(ROOT, "rigidfibers_kth_b200", "mlp_weights.npy"))
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison arm")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- product arm
+def make_sim(rf, pos, ori, device, precision, pc, velocity_mode, tol=WORKLOAD["tol"]):
+    p = rf.FiberParams(slenderness=WORKLOAD["eps"], timestep=WORKLOAD["dt"],
+                       num_terms_in_force_expansion=WORKLOAD["N"], num_quadrature_intervals=WORKLOAD["NoQI"],
+                       gmres_restart=WORKLOAD["restart"], gmres_tol=tol, gmres_max_iters=300,
+                       precision=precision, preconditioner=pc, velocity_mode=velocity_mode, device=device)
+    return rf.Simulation(rf.Configuration(p, pos, ori))
+
+
+def timed_steps(sim, steps, warmup, world, first_index=0):
+    """Device time of `steps` steps after `warmup` untimed ones (marker 0 -> 1)."""
+    t = first_index
+    for _ in range(warmup):
+        sim.step(t)
+        t += 1
+    barrier(world)
+    launches0 = sim.kernel_launches()
+    sim.mark(0)
+    for _ in range(steps):
+        sim.step(t)
+        t += 1
+    sim.mark(1)
+    ms = sim.elapsed_ms(0, 1)
+    launches = sim.kernel_launches() - launches0
+    barrier(world)
+    return ms, launches, t
+
+
+def phase_breakdown(sim, t):
+    sim.mark(2)
+    sim.assemble_system()
+    sim.mark(3)
+    sim.solve_system()
+    sim.mark(4)
+    sim.update_velocities()
+    sim.mark(5)
+    sim.update_fibers(t == 0)
+    sim.mark(6)
+    return dict(assemble=sim.elapsed_ms(2, 3), solve=sim.elapsed_ms(3, 4), velocities=sim.elapsed_ms(4, 5),
+                advect=sim.elapsed_ms(5, 6))
+
+
+def cpu_baseline_sample(pos, ori, matvecs):
+    """Oracle (OpenMP FP64 restatement of the reference Fortran) on a bounded
+    sample: the rows of S target fibers for assembly and velocities (all 4000
+    sources) and `matvecs` products with those rows; scaled by M/S."""
+    from oracle import rfo
+
+    M = len(pos)
+    S = max(1, min(M, 200 * M // 4000))
+    p = rfo.make_params(M, N=WORKLOAD["N"], NoQI=WORKLOAD["NoQI"], eps=WORKLOAD["eps"], dt=WORKLOAD["dt"])
+    t0 = time.perf_counter()
+    A, _ = rfo.assemble_rows(p, pos, ori, 0, S)
+    t1 = time.perf_counter()
+    x = np.ones(A.shape[1]) * 1e-3
+    for _ in range(matvecs):
+        rfo.matvec_rect(A, x)
+    t2 = time.perf_counter()
+    rfo.velocities_rows(p, pos, ori, np.zeros(A.shape[1]), 0, S)
+    t3 = time.perf_counter()
+    sample_s = t3 - t0
+    step_s = sample_s * M / S
+    return {"value": 1.0 / step_s, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"rows of {S} of {M} target fibers: assembly {t1 - t0:.2f}s, {matvecs} FP64 row matvecs "
+                      f"{t2 - t1:.2f}s, velocities {t3 - t2:.2f}s; scaled by M/S = {M / S:.0f}"}
+
+
+def run_ours(args):
+    world, rank, local = dist_setup()
+    import rigidfibers_kth_b200 as rf
+
+    M = args.M
+    pos, ori = rf.generate_layout(M, WORKLOAD["distribution"], WORKLOAD["box"], WORKLOAD["min_dist"],
+                                  seed=WORKLOAD["seed"] + rank)
+    prec = rf.PREC_MIXED_BF16 if args.precision == "bf16" else rf.PREC_MIXED_FP32
+    pc = {"none": rf.PC_NONE, "cluster": rf.PC_CLUSTER, "learned": rf.PC_LEARNED}[args.pc]
+    sim = make_sim(rf, pos, ori, local, prec, pc, rf.VEL_REUSE)
+    if pc == rf.PC_LEARNED:
+        sim.set_mlp_weights(np.load(args.weights))
+    clocks = ClockSampler(local)
+    # warm-up, then the timed region with clock sampling
+    t = 0
+    for _ in range(args.warmup):
+        sim.step(t)
+        t += 1
+    barrier(world)
+    clocks.start()
+    launches0 = sim.kernel_launches()
+    sim.mark(0)
+    stats = []
+    for _ in range(args.steps):
+        sim.step(t)
+        stats.append(sim.solve_stats())
+        t += 1
+    sim.mark(1)
+    ms = sim.elapsed_ms(0, 1)
+    launches = sim.kernel_launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    ms = max_over_ranks(ms, world)
+    value = world * args.steps / (ms * 1e-3)
+
+    # end to end through the public API with host buffers: upload the state,
+    # step, download velocities and state, every step
+    import ctypes
+
+    hp, ho = sim.state()
+    hp = np.ascontiguousarray(hp)
+    ho = np.ascontiguousarray(ho)
+    barrier(world)
+    sim.mark(7)
+    for _ in range(args.steps):
+        sim.set_state(hp, ho)
+        sim.step(t)
+        t += 1
+        v, w = sim.velocities()
+        hp, ho = sim.state()
+    sim.mark(8)
+    e2e_ms = max_over_ranks(sim.elapsed_ms(7, 8), world)
+    e2e_value = world * args.steps / (e2e_ms * 1e-3)
+    phases = phase_breakdown(sim, t)
+    t += 1
+    mv_ms, mv_bytes = sim.profile_matvec(reps=10)
+    solve_stats = stats[-1]
+
+    out = None
+    if rank == 0:
+        # plain FP64 GPU path (the reference method) and the velocity error
+        plain = None
+        verr = None
+        if not args.no_plain:
+            sim64 = make_sim(rf, pos, ori, local, rf.PREC_FP64, rf.PC_NONE, rf.VEL_RECOMPUTE)
+            ms64, l64, _ = timed_steps(sim64, max(1, min(args.steps, 3)), 1, 1)
+            plain = {"value": max(1, min(args.steps, 3)) / (ms64 * 1e-3), "unit": "steps/s",
+                     "ms_per_step": ms64 / max(1, min(args.steps, 3))}
+            plain["phases_ms"] = phase_breakdown(sim64, 99)
+            plain["matvecs_per_step"] = sim64.solve_stats()["matvecs"]
+            sim64.close()
+            # velocity error of the product path against FP64 on the initial layout
+            ref = make_sim(rf, pos, ori, local, rf.PREC_FP64, rf.PC_NONE, rf.VEL_RECOMPUTE, tol=1e-12)
+            ref.assemble_system(); ref.solve_system(); ref.update_velocities()
+            V64, W64 = ref.velocities()
+            ref.close()
+            chk = make_sim(rf, pos, ori, local, prec, pc, rf.VEL_REUSE)
+            if pc == rf.PC_LEARNED:
+                chk.set_mlp_weights(np.load(args.weights))
+            chk.assemble_system(); chk.solve_system(); chk.update_velocities()
+            V, W = chk.velocities()
+            chk.close()
+            verr = {"translational": float(np.abs(V - V64).max() / np.abs(V64).max()),
+                    "rotational": float(np.abs(W - W64).max() / np.abs(W64).max()),
+                    "bound": 1e-6, "norm": "max over fibers / max |FP64 velocity|"}
+        # roofline of the dominant kernel
+        solve_share = phases["solve"]
+        if phases["assemble"] >= solve_share:
+            dominant = "assemble_kernel"
+        else:
+            dominant = "gemv_partial_kernel (BF16 A, inner GMRES)"
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+            os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        roof = {"bound": "hbm", "kernel": "gemv_partial_kernel + gemv_reduce_kernel (BF16 A x FP32 x)",
+                "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm_peak,
+                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes": mv_bytes, "ms_per_launch": mv_ms,
+                "dominant_phase": dominant}
+        cpu = None if args.no_cpu else cpu_baseline_sample(pos, ori, FP64_MATVECS_PER_STEP)
+        n = 3 * WORKLOAD["N"] * M
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "bf16+fp32+fp64",
+            "data": "synthetic",
+            "config": {
+                "workload": f"M={M} fibers, clustered cloud (Gaussian centres sigma {WORKLOAD['box']}, min centre "
+                            f"distance {WORKLOAD['min_dist']}), eps {WORKLOAD['eps']}, N={WORKLOAD['N']}, "
+                            f"8x3 Gauss points, dt {WORKLOAD['dt']}, GMRES({WORKLOAD['restart']}) to an FP64 "
+                            f"residual of {WORKLOAD['tol']}",
+                "system": f"{n} x {n} dense", "precision": args.precision + " A + FP64 refinement",
+                "preconditioner": args.pc, "velocities": "stored P0/P1 projection panels",
+                "l2": "inputs larger than L2 (BF16 A {:.1f} GB, FP32 A {:.1f} GB)".format(n * n * 2e-9, n * n * 4e-9),
+                "parallelism": f"replicas x{world}",
+            },
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 2 * 3 * M * 8,
+                    "d2h_bytes_per_step": 4 * 3 * M * 8},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "phases_ms": phases,
+            "solve": solve_stats,
+            "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (value / world) / plain["value"] if plain else None,
+            "velocity_error": verr,
+        }
+    sim.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return out
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    import rigidfibers_kth_b200 as rf
+
+    M = args.M
+    pos, ori = rf.generate_layout(M, WORKLOAD["distribution"], WORKLOAD["box"], WORKLOAD["min_dist"],
+                                  seed=WORKLOAD["seed"])
+    samples = []
+    for _ in range(args.warmup):
+        cpu_baseline_sample(pos, ori, FP64_MATVECS_PER_STEP)
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline_sample(pos, ori, FP64_MATVECS_PER_STEP)
+        samples.append(1.0 / last["value"])
+    step_s = float(np.mean(samples))
+    value = 1.0 / step_s
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_s * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"M={M} fibers, clustered cloud; reference method in FP64 on the host cores",
+                   "parallelism": "OpenMP threads on the host"},
+        "cpu_baseline": {"value": value, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": last["sample"] if last else ""},
+        "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

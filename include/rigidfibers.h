@@ -98,7 +98,8 @@ typedef struct rf_params {
     int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 12) */
     double inner_tol;                    /* mixed precision: inner GMRES relative tolerance (default 1e-3) */
     double near_field_c;                 /* mixed precision: squared distance below which the analytic
-                                            integral stays FP64 (default 10, the recursion switch) */
+                                            integral stays FP64 (default 10, the recursion switch);
+                                            >= 1e30 keeps every integral in FP64 */
     int32_t reserved[8];
 } rf_params;
 
@@ -153,6 +154,16 @@ rf_status rf_get_history(rf_handle *h, double *prev_pos, double *prev_orient, do
                          double *prev_rot);
 rf_status rf_set_history(rf_handle *h, const double *prev_pos, const double *prev_orient,
                          const double *prev_vel, const double *prev_rot, const double *coeffs);
+
+/* Device-time markers on the handle's stream (replaces the cudaEvent timer of
+ * src/performance.cc:31-65): record marker slot 0..15; elapsed milliseconds
+ * between two recorded slots (waits for the later one).  Returns < 0 on error. */
+rf_status rf_timer_mark(rf_handle *h, int32_t slot);
+double rf_timer_elapsed_ms(rf_handle *h, int32_t from, int32_t to);
+/* Average device time of one matrix-vector product with the stored matrix in
+ * the precision the inner GMRES uses (FP64, FP32 or BF16), over reps launches
+ * on device-resident vectors; bytes of A streamed per product in *bytes. */
+rf_status rf_profile_matvec(rf_handle *h, int32_t reps, double *ms_per_product, double *bytes);
 
 /* Sizes. */
 int64_t rf_system_size(const rf_handle *h);   /* n = 3*N*M */

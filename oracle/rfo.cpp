@@ -535,22 +535,26 @@ int rfo_solve_direct(int n, double *A, double *x) {
     return 0;
 }
 
-void rfo_matvec(int n, const double *A, const double *x, double *y, int threads) {
+void rfo_matvec_rect(int m, int n, const double *A, long long lda, const double *x, double *y, int threads) {
     // dgemv('N') order: y_i = sum_j A_ij x_j accumulated over j in order.
     set_threads(threads);
     const int RB = 256;
 #pragma omp parallel for schedule(static)
-    for (int r0 = 0; r0 < n; r0 += RB) {
-        const int r1 = std::min(n, r0 + RB);
+    for (int r0 = 0; r0 < m; r0 += RB) {
+        const int r1 = std::min(m, r0 + RB);
         double acc[256];
         for (int r = r0; r < r1; ++r) acc[r - r0] = 0.0;
         for (int c = 0; c < n; ++c) {
             const double xc = x[c];
-            const double *col = A + (size_t)c * n;
+            const double *col = A + (size_t)c * lda;
             for (int r = r0; r < r1; ++r) acc[r - r0] += xc * col[r];
         }
         for (int r = r0; r < r1; ++r) y[r] = acc[r - r0];
     }
+}
+
+void rfo_matvec(int n, const double *A, const double *x, double *y, int threads) {
+    rfo_matvec_rect(n, n, A, n, x, y, threads);
 }
 
 static double dot(int n, const double *a, const double *b) {

@@ -60,6 +60,8 @@ int rfo_solve_gmres(int n, const double *A, const double *b, double *x,
                     int *iters, double *backward_error, int threads);
 /* y = A x (column-major, dgemv 'N' order) */
 void rfo_matvec(int n, const double *A, const double *x, double *y, int threads);
+/* y = A x for an m x n column-major A with leading dimension lda */
+void rfo_matvec_rect(int m, int n, const double *A, long long lda, const double *x, double *y, int threads);
 /* coeffs_and_vels.f90:543-746 */
 int rfo_velocities(const rfo_params *p, const double *X, const double *T,
                    const double *coeffs, double *V, double *W);

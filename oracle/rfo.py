@@ -56,6 +56,8 @@ def lib():
                                       ctypes.c_double, _ip, _dp, ctypes.c_int]
         L.rfo_matvec.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_int]
         L.rfo_matvec.restype = None
+        L.rfo_matvec_rect.argtypes = [ctypes.c_int, ctypes.c_int, _dp, ctypes.c_longlong, _dp, _dp, ctypes.c_int]
+        L.rfo_matvec_rect.restype = None
         L.rfo_velocities.argtypes = [ctypes.POINTER(RfoParams), _dp, _dp, _dp, _dp, _dp]
         L.rfo_velocities_rows.argtypes = [ctypes.POINTER(RfoParams), _dp, _dp, _dp, ctypes.c_int,
                                           ctypes.c_int, _dp, _dp]
@@ -148,6 +150,14 @@ def matvec(A, x, threads=0):
     x = np.ascontiguousarray(x, dtype=np.float64)
     y = np.zeros_like(x)
     lib().rfo_matvec(len(x), _ptr(A), _ptr(x), _ptr(y), threads)
+    return y
+
+
+def matvec_rect(A, x, threads=0):
+    A = np.asfortranarray(A, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(A.shape[0])
+    lib().rfo_matvec_rect(A.shape[0], A.shape[1], _ptr(A), A.shape[0], _ptr(x), _ptr(y), threads)
     return y
 
 

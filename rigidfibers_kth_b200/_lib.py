@@ -123,6 +123,9 @@ def lib():
         "rf_get_solve_stats": (ctypes.c_int, [_h, ctypes.POINTER(RfSolveStats)]),
         "rf_get_history": (ctypes.c_int, [_h, _dp, _dp, _dp, _dp]),
         "rf_set_history": (ctypes.c_int, [_h, _dp, _dp, _dp, _dp, _dp]),
+        "rf_timer_mark": (ctypes.c_int, [_h, ctypes.c_int32]),
+        "rf_timer_elapsed_ms": (ctypes.c_double, [_h, ctypes.c_int32, ctypes.c_int32]),
+        "rf_profile_matvec": (ctypes.c_int, [_h, ctypes.c_int32, _dp, _dp]),
         "rf_system_size": (ctypes.c_int64, [_h]),
         "rf_matrix_ld": (ctypes.c_int64, [_h]),
         "rf_get_stream": (ctypes.c_void_p, [_h]),

@@ -38,6 +38,8 @@ void free_all(rf_handle *h) {
     h->gm64.reset();
     h->gm32.reset();
     if (h->hscal) cudaFreeHost(h->hscal);
+    for (auto &ev : h->marks)
+        if (ev) cudaEventDestroy(ev);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -402,7 +404,9 @@ rf_status rf_assemble_system(rf_handle *h) {
         a.near_c = h->p.near_field_c > 0.0 ? h->p.near_field_c : 10.0;
         a.axis_ratio = 1.0 / 16.0;
     }
-    const int pmode = prec == RF_PREC_FP64 ? rf::kPModeFP64 : rf::kPModeMixed;
+    // near_field_c >= 1e30 keeps every integral in FP64 for the mixed paths
+    const int pmode = (prec == RF_PREC_FP64 || (prec != RF_PREC_FP32 && a.near_c >= 1e30)) ? rf::kPModeFP64
+                                                                                          : rf::kPModeMixed;
     CK(h, rf::launch_assemble(a, h->p.use_analytical_integration == 0, pmode, h->asm_chunks, h->stream),
        "assemble kernel");
     CK(h, rf::launch_reduce_chunks(h->bpart, h->asm_chunks, h->n, h->n, h->b, h->stream), "rhs reduction");
@@ -742,6 +746,63 @@ rf_status rf_set_history(rf_handle *h, const double *prev_pos, const double *pre
     if (prev_vel) CK(h, cudaMemcpy(h->V[h->vprev], prev_vel, m3, cudaMemcpyHostToDevice), "upload");
     if (prev_rot) CK(h, cudaMemcpy(h->W[h->vprev], prev_rot, m3, cudaMemcpyHostToDevice), "upload");
     if (coeffs) CK(h, cudaMemcpy(h->x, coeffs, h->n * 8, cudaMemcpyHostToDevice), "upload");
+    return RF_OK;
+}
+
+rf_status rf_timer_mark(rf_handle *h, int32_t slot) {
+    if (!h || slot < 0 || slot >= 16) return rf::fail(h, RF_ERR_INVALID_ARG, "timer slot must be 0..15");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    if (!h->marks[slot]) CK(h, cudaEventCreate(&h->marks[slot]), "event");
+    CK(h, cudaEventRecord(h->marks[slot], h->stream), "event record");
+    return RF_OK;
+}
+
+double rf_timer_elapsed_ms(rf_handle *h, int32_t from, int32_t to) {
+    if (!h || from < 0 || from >= 16 || to < 0 || to >= 16 || !h->marks[from] || !h->marks[to]) return -1.0;
+    if (cudaSetDevice(h->device) != cudaSuccess) return -1.0;
+    if (cudaEventSynchronize(h->marks[to]) != cudaSuccess) return -1.0;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->marks[from], h->marks[to]) != cudaSuccess) return -1.0;
+    return ms;
+}
+
+rf_status rf_profile_matvec(rf_handle *h, int32_t reps, double *ms_per_product, double *bytes) {
+    if (!h || reps < 1 || !ms_per_product) return rf::fail(h, RF_ERR_INVALID_ARG, "bad argument");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    const int64_t n = h->n;
+    void *xv = nullptr, *yv = nullptr;
+    CK(h, cudaMalloc(&xv, n * 8), "alloc");
+    cudaError_t e = cudaMalloc(&yv, n * 8);
+    if (e == cudaSuccess) e = cudaMemsetAsync(xv, 0, n * 8, h->stream);
+    double elem = 8.0;
+    if (e == cudaSuccess) e = cudaEventRecord(h->ev0, h->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        if (h->A64) {
+            e = rf::launch_gemv<double, double, double, double>(h->A64, h->lda, n, n, (double *)xv, (double *)yv,
+                                                                nullptr, h->work64, h->work_elems, h->sm_count,
+                                                                h->stream);
+            elem = 8.0;
+        } else if (h->A16) {
+            e = rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, n, n, (float *)xv, (float *)yv,
+                                                                    nullptr, h->work32, h->work_elems, h->sm_count,
+                                                                    h->stream);
+            elem = 2.0;
+        } else {
+            e = rf::launch_gemv<float, float, float, float>(h->A32, h->lda, n, n, (float *)xv, (float *)yv, nullptr,
+                                                            h->work32, h->work_elems, h->sm_count, h->stream);
+            elem = 4.0;
+        }
+        h->launches += 2;
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(h->ev1, h->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(h->ev1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    cudaFree(xv);
+    cudaFree(yv);
+    CK(h, e, "profile matvec");
+    *ms_per_product = ms / reps;
+    if (bytes) *bytes = elem * (double)h->lda * (double)n;
     return RF_OK;
 }
 

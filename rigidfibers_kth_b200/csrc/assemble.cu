@@ -59,12 +59,12 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
     double *s_wP = s_pv + kMaxLQ;                           // 16 x kMaxLQ : w_q P_m(q), rows > N zero
     double *s_xt = s_wP + 16 * kMaxLQ;                      // TI x 3
     double *s_tt = s_xt + TI * 3;                           // TI x 3
-    double *s_acc = s_tt + TI * 3;                          // TI x (3N + 6) running sums
-    double *s_th = s_acc + TI * (3 * N + 6);                // TI x NL(k) x NG
+    double *s_acc = s_tt + TI * 3;                          // TI x NL(k) x 6: sum_j theta^k_0
+    double *s_th = s_acc + TI * NL * 6;                     // TI x NL(k) x NG
     // the tensor values of P1/P2 and the staged block of P3 share one region
     double *s_G = s_th + TI * NL * NG;                      // NCOL x LDQ
     double *s_blk = s_G;                                    // CT x RT staged block
-    const int big = max(NCOL * LDQ, CT * RT);
+    const int big = max(NCOL * LDQ, CT * RT + 2 * CT * TI * 3);
     float *s_pvf = reinterpret_cast<float *>(s_G + big);    // kMaxLQ
     float *s_wPf = s_pvf + kMaxLQ;                          // NL x kMaxLQ
 
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
         s_xt[t] = (i < a.M) ? a.pos[3 * i + c] : 0.0;
         s_tt[t] = (i < a.M) ? a.ori[3 * i + c] : 1.0;
     }
-    for (int t = tid; t < TI * (3 * N + 6); t += nthreads) s_acc[t] = 0.0;
+    for (int t = tid; t < TI * NL * 6; t += nthreads) s_acc[t] = 0.0;
     __syncthreads();
 
     const bool worker = tid < nwork;
@@ -118,24 +118,18 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
     const int64_t rows_left = (int64_t)a.M * 3 * N - row0;
     const int rows_valid = rows_left < (int64_t)RT ? (int)rows_left : RT;
 
+    __shared__ int s_nlist;
+    __shared__ short s_list[kTI * kMaxLQ];
+
     for (int j = j0; j < j1; ++j) {
         // ---------------- P1: inner integral at (target point, source j)
-        if (worker) {
-            const double xs0 = __ldg(a.pos + 3 * j), xs1 = __ldg(a.pos + 3 * j + 1), xs2 = __ldg(a.pos + 3 * j + 2);
-            const double ts0 = __ldg(a.ori + 3 * j), ts1 = __ldg(a.ori + 3 * j + 1), ts2 = __ldg(a.ori + 3 * j + 2);
-            double *g = s_G + (size_t)ti * NG * LDQ + qpos;
-            if (i < a.M && i != j) {
-                const double r0x = fsub(xbx, xs0), r0y = fsub(xby, xs1), r0z = fsub(xbz, xs2);
-                bool use64 = true;
-                if (PMODE == kPModeMixed) {
-                    // FP64 near the source fiber (c < near_c) and close to its axis
-                    // beyond the ends (d < c * axis_ratio), FP32 elsewhere
-                    const double bq = -2.0 * (ts0 * r0x + ts1 * r0y + ts2 * r0z);
-                    const double cq = r0x * r0x + r0y * r0y + r0z * r0z;
-                    const double dq = cq - 0.25 * bq * bq;
-                    use64 = NUMERIC ? (cq < a.near_c) : (cq < a.near_c || dq < cq * a.axis_ratio);
-                }
-                if (use64) {
+        const double xs0 = __ldg(a.pos + 3 * j), xs1 = __ldg(a.pos + 3 * j + 1), xs2 = __ldg(a.pos + 3 * j + 2);
+        const double ts0 = __ldg(a.ori + 3 * j), ts1 = __ldg(a.ori + 3 * j + 1), ts2 = __ldg(a.ori + 3 * j + 2);
+        if (PMODE == kPModeFP64) {
+            if (worker) {
+                double *g = s_G + (size_t)ti * NG * LDQ + qpos;
+                if (i < a.M && i != j) {
+                    const double r0x = fsub(xbx, xs0), r0y = fsub(xby, xs1), r0z = fsub(xbz, xs2);
                     if (NUMERIC) {
                         double G[NL][6];
                         const double xs[3] = {xs0, xs1, xs2}, ts[3] = {ts0, ts1, ts2};
@@ -148,24 +142,78 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
                         inner_analytic_store_fp64<N>(r0x, r0y, r0z, ts0, ts1, ts2, eps2, g, LDQ);
                     }
                 } else {
-                    if (NUMERIC) {
-                        float G[NL][6];
-                        const float xs[3] = {(float)xs0, (float)xs1, (float)xs2};
-                        const float ts[3] = {(float)ts0, (float)ts1, (float)ts2};
-                        inner_numeric_fp32<N>((float)xbx, (float)xby, (float)xbz, xs, ts, s_pvf, s_wPf, LQ,
-                                              (float)eps2, G);
 #pragma unroll
-                        for (int m = 0; m < NL; ++m)
-#pragma unroll
-                            for (int c = 0; c < 6; ++c) g[(m * 6 + c) * LDQ] = (double)G[m][c];
-                    } else {
-                        inner_analytic_store_fp32<N>((float)r0x, (float)r0y, (float)r0z, (float)ts0, (float)ts1,
-                                                     (float)ts2, (float)eps2, g, LDQ);
-                    }
+                    for (int m = 0; m < NG; ++m) g[m * LDQ] = 0.0;
                 }
-            } else {
+            }
+        } else {
+            // Mixed precision in two passes: FP32 for the far field, then the
+            // points near the source fiber (c < near_c) or close to its axis
+            // beyond the ends (d < c * axis_ratio) in FP64, compacted onto
+            // consecutive threads so that no warp carries both paths.
+            if (tid == 0) s_nlist = 0;
+            __syncthreads();
+            if (worker) {
+                double *g = s_G + (size_t)ti * NG * LDQ + qpos;
+                bool need64 = false;
+                if (i < a.M && i != j) {
+                    const double r0x = xbx - xs0, r0y = xby - xs1, r0z = xbz - xs2;
+                    const double bq = -2.0 * (ts0 * r0x + ts1 * r0y + ts2 * r0z);
+                    const double cq = r0x * r0x + r0y * r0y + r0z * r0z;
+                    const double dq = cq - 0.25 * bq * bq;
+                    need64 = NUMERIC ? (cq < a.near_c) : (cq < a.near_c || dq < cq * a.axis_ratio);
+                    if (!need64) {
+                        if (NUMERIC) {
+                            float G[NL][6];
+                            const float xs[3] = {(float)xs0, (float)xs1, (float)xs2};
+                            const float ts[3] = {(float)ts0, (float)ts1, (float)ts2};
+                            inner_numeric_fp32<N>((float)xbx, (float)xby, (float)xbz, xs, ts, s_pvf, s_wPf, LQ,
+                                                  (float)eps2, G);
 #pragma unroll
-                for (int m = 0; m < NG; ++m) g[m * LDQ] = 0.0;
+                            for (int m = 0; m < NL; ++m)
+#pragma unroll
+                                for (int c = 0; c < 6; ++c) g[(m * 6 + c) * LDQ] = (double)G[m][c];
+                        } else {
+                            inner_analytic_store_fp32<N>((float)r0x, (float)r0y, (float)r0z, (float)ts0, (float)ts1,
+                                                         (float)ts2, (float)eps2, g, LDQ);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int m = 0; m < NG; ++m) g[m * LDQ] = 0.0;
+                }
+                // warp-aggregated append of the FP64 items
+                const unsigned mask = __ballot_sync(__activemask(), need64);
+                if (mask) {
+                    int base = 0;
+                    const int leader = __ffs(mask) - 1;
+                    if (lane == leader) base = atomicAdd(&s_nlist, __popc(mask));
+                    base = __shfl_sync(__activemask(), base, leader);
+                    if (need64) s_list[base + __popc(mask & ((1u << lane) - 1u))] = (short)tid;
+                }
+            }
+            __syncthreads();
+            const int nl = s_nlist;
+            for (int u = tid; u < nl; u += nthreads) {
+                const int item = s_list[u];
+                const int ti2 = item / LQ, q2 = item - ti2 * LQ;
+                const double sq2 = s_pv[q2];
+                const double bx = fadd(s_xt[ti2 * 3 + 0], fmul(sq2, s_tt[ti2 * 3 + 0]));
+                const double by = fadd(s_xt[ti2 * 3 + 1], fmul(sq2, s_tt[ti2 * 3 + 1]));
+                const double bz = fadd(s_xt[ti2 * 3 + 2], fmul(sq2, s_tt[ti2 * 3 + 2]));
+                double *g2 = s_G + (size_t)ti2 * NG * LDQ + (q2 & 3) * KS + (q2 >> 2);
+                if (NUMERIC) {
+                    double G[NL][6];
+                    const double xs[3] = {xs0, xs1, xs2}, ts[3] = {ts0, ts1, ts2};
+                    inner_numeric_fp64<N>(bx, by, bz, xs, ts, s_pv, s_wP, LQ, eps2, G);
+#pragma unroll
+                    for (int m = 0; m < NL; ++m)
+#pragma unroll
+                        for (int c = 0; c < 6; ++c) g2[(m * 6 + c) * LDQ] = G[m][c];
+                } else {
+                    inner_analytic_store_fp64<N>(fsub(bx, xs0), fsub(by, xs1), fsub(bz, xs2), ts0, ts1, ts2, eps2, g2,
+                                                 LDQ);
+                }
             }
         }
         // q padding up to the next multiple of 4 is zero for the tensor-core k-steps
@@ -242,56 +290,51 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
 #pragma unroll
                 for (int aa = 0; aa < 3; ++aa) s_blk[(cl + bb) * RT + rl + aa] = v[aa][bb];
         }
-        // right-hand side and the l = 0 velocity terms, one owner thread per accumulator
-        for (int t = tid; t < TI * (3 * N + 6); t += nthreads) {
-            const int gt = t / (3 * N + 6);
-            const int r = t - gt * (3 * N + 6);
-            if (i0 + gt >= a.M || i0 + gt == j) continue;
-            if (r >= 3 * N && !a.vpart) continue;
-            const double *tt = s_tt + gt * 3;
-            const double *f = tab.half_force;
-            const int k = r < 3 * N ? r / 3 + 1 : (r - 3 * N) / 3;
-            const int aa = r % 3;
-            const double *th = s_th + ((size_t)gt * NL + k) * NG;  // l = 0
-            double contr[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                contr[c] = th[sym_index(c, 0)] * f[0] + th[sym_index(c, 1)] * f[1] + th[sym_index(c, 2)] * f[2];
-            const double tdc = tt[0] * contr[0] + tt[1] * contr[1] + tt[2] * contr[2];
-            if (r < 3 * N) {
-                if (k == 1) s_acc[t] -= tab.D1 * tdc * tt[aa];
-                else s_acc[t] -= tab.gamma[k] * (contr[aa] - tab.Ek[k] * tdc * tt[aa]);
-            } else if (k == 0) {
-                s_acc[t] += 0.5 / tab.d * contr[aa];
-            } else {
-                s_acc[t] += 1.5 / tab.d * (contr[aa] - tdc * tt[aa]);
-            }
+        // right-hand side and the l = 0 velocity terms: the external force is the
+        // same on every fiber, so theta^k_0 is summed over the sources here and
+        // contracted with 0.5*ExtForce once at the end
+        for (int t = tid; t < TI * NL * 6; t += nthreads) {
+            const int gt = t / (NL * 6);
+            const int r = t - gt * (NL * 6);
+            if (i0 + gt == j) continue;
+            s_acc[t] += s_th[((size_t)gt * NL + r / 6) * NG + r % 6];
         }
-        // velocity panels: rows i*3 + aa of PV (P_0) and PW (P_1, projected)
+        // velocity panels: rows i*3 + aa of PV (P_0) and PW (P_1, projected),
+        // per (target, l) group into the staging area after the block
         if (a.PV64 || a.PV32) {
-            constexpr int PRT = TI * 3;
-            const int64_t prow0 = (int64_t)i0 * 3;
-            const int64_t col0 = (int64_t)j * 3 * N;
-            for (int e = tid; e < CT * PRT; e += nthreads) {
-                const int cl = e / PRT;
-                const int rl = e - cl * PRT;
-                const int gt = rl / 3, aa = rl % 3;
-                if (i0 + gt >= a.M) continue;
-                const int l = cl / 3 + 1, bb = cl % 3;
-                double pv = 0.0, pw = 0.0;
+            double *s_pan = s_blk + CT * RT;   // [2][CT][TI*3]
+            for (int g = tid; g < TI * N; g += nthreads) {
+                const int l = g / TI + 1, gt = g - (l - 1) * TI;
+                double pv[3][3], pw[3][3];
                 if (i0 + gt != j) {
                     const double *th0 = s_th + ((size_t)gt * NL + 0) * NG + l * 6;
                     const double *th1 = s_th + ((size_t)gt * NL + 1) * NG + l * 6;
                     const double *tt = s_tt + gt * 3;
-                    pv = 0.5 / tab.d * th0[sym_index(aa, bb)];
-                    double tdot = 0.0;
+                    const double sv = 0.5 / tab.d, sw = 1.5 / tab.d;
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) tdot += tt[c] * th1[sym_index(c, bb)];
-                    pw = 1.5 / tab.d * (th1[sym_index(aa, bb)] - tdot * tt[aa]);
+                    for (int bb = 0; bb < 3; ++bb) {
+                        const double tdot = tt[0] * th1[sym_index(0, bb)] + tt[1] * th1[sym_index(1, bb)] +
+                                            tt[2] * th1[sym_index(2, bb)];
+#pragma unroll
+                        for (int aa = 0; aa < 3; ++aa) {
+                            pv[aa][bb] = sv * th0[sym_index(aa, bb)];
+                            pw[aa][bb] = sw * (th1[sym_index(aa, bb)] - tdot * tt[aa]);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa)
+#pragma unroll
+                        for (int bb = 0; bb < 3; ++bb) pv[aa][bb] = pw[aa][bb] = 0.0;
                 }
-                const int64_t idx = (col0 + cl) * a.ldp + prow0 + rl;
-                if (a.PV64) { a.PV64[idx] = pv; a.PW64[idx] = pw; }
-                if (a.PV32) { a.PV32[idx] = (float)pv; a.PW32[idx] = (float)pw; }
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa) {
+                        const int cl = 3 * (l - 1) + bb, rl = gt * 3 + aa;
+                        s_pan[cl * (TI * 3) + rl] = pv[aa][bb];
+                        s_pan[CT * TI * 3 + cl * (TI * 3) + rl] = pw[aa][bb];
+                    }
             }
         }
         __syncthreads();
@@ -318,17 +361,53 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
                     if (a.A16) a.A16[idx] = __float2bfloat16_rn((float)v0);
                 }
             }
+            if (a.PV64 || a.PV32) {
+                constexpr int PRT = TI * 3;
+                const double *s_pan = s_blk + CT * RT;
+                const int prows = min(PRT, 3 * (a.M - i0));
+                const int64_t prow0 = (int64_t)i0 * 3;
+                for (int e = tid; e < 2 * CT * PRT; e += nthreads) {
+                    const int which = e / (CT * PRT);
+                    const int r = e - which * CT * PRT;
+                    const int cl = r / PRT, rl = r - cl * PRT;
+                    if (rl >= prows) continue;
+                    const int64_t idx = (col0 + cl) * a.ldp + prow0 + rl;
+                    const double v = s_pan[e];
+                    if (a.PV64) (which ? a.PW64 : a.PV64)[idx] = v;
+                    if (a.PV32) (which ? a.PW32 : a.PV32)[idx] = (float)v;
+                }
+            }
         }
         __syncthreads();  // the staged block and the next P1 share shared memory
     }
-    // per-chunk partial sums: rhs [chunk][n], velocity l=0 terms [chunk][6M]
+    // per-chunk partial sums: rhs [chunk][n] and velocity l=0 terms [chunk][6M]
+    // from sum_j theta^k_0 (matrix_assembly.f90:874-899)
     for (int t = tid; t < TI * (3 * N + 6); t += nthreads) {
         const int gt = t / (3 * N + 6);
         const int r = t - gt * (3 * N + 6);
         const int ii = i0 + gt;
         if (ii >= a.M) continue;
-        if (r < 3 * N) a.bpart[(int64_t)blockIdx.y * a.n + (int64_t)ii * 3 * N + r] = s_acc[t];
-        else if (a.vpart) a.vpart[(int64_t)blockIdx.y * 6 * a.M + (int64_t)ii * 6 + (r - 3 * N)] = s_acc[t];
+        if (r >= 3 * N && !a.vpart) continue;
+        const double *tt = s_tt + gt * 3;
+        const double *f = tab.half_force;
+        const int k = r < 3 * N ? r / 3 + 1 : (r - 3 * N) / 3;
+        const int aa = r % 3;
+        const double *th = s_acc + (gt * NL + k) * 6;
+        double contr[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            contr[c] = th[sym_index(c, 0)] * f[0] + th[sym_index(c, 1)] * f[1] + th[sym_index(c, 2)] * f[2];
+        const double tdc = tt[0] * contr[0] + tt[1] * contr[1] + tt[2] * contr[2];
+        double v;
+        if (r < 3 * N) {
+            if (k == 1) v = -tab.D1 * tdc * tt[aa];
+            else v = -tab.gamma[k] * (contr[aa] - tab.Ek[k] * tdc * tt[aa]);
+            a.bpart[(int64_t)blockIdx.y * a.n + (int64_t)ii * 3 * N + r] = v;
+        } else {
+            if (k == 0) v = 0.5 / tab.d * contr[aa];
+            else v = 1.5 / tab.d * (contr[aa] - tdc * tt[aa]);
+            a.vpart[(int64_t)blockIdx.y * 6 * a.M + (int64_t)ii * 6 + (r - 3 * N)] = v;
+        }
     }
 }
 
@@ -346,8 +425,8 @@ static cudaError_t launch_assemble_n(const AsmArgs &a, int nchunks, cudaStream_t
     constexpr int TI = kTI;
     constexpr int NL = N + 1, NG = NL * 6;
     const int LQ = a.LQ, LDQ = round_up_int(LQ, 4) + 2;
-    const size_t big = std::max((size_t)TI * NG * LDQ, (size_t)(3 * N) * (TI * 3 * N));
-    size_t smem = sizeof(double) * (kMaxLQ + 16 * kMaxLQ + TI * 3 * 2 + TI * (3 * N + 6) + TI * NL * NG + big);
+    const size_t big = std::max((size_t)TI * NG * LDQ, (size_t)(3 * N) * (TI * 3 * N) + 2 * (3 * N) * (TI * 3));
+    size_t smem = sizeof(double) * (kMaxLQ + 16 * kMaxLQ + TI * 3 * 2 + TI * NL * 6 + TI * NL * NG + big);
     smem += sizeof(float) * (kMaxLQ + NL * kMaxLQ);
     const int threads = round_up_int(TI * LQ, 32);
     auto kern = threads <= 96 ? assemble_kernel<N, NUMERIC, PMODE, 96, kMinBlocks96>

@@ -21,6 +21,7 @@ struct rf_handle {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t marks[16] = {};
 
     // state: positions/orientations triple-buffered, velocities double-buffered
     double *X[3] = {nullptr, nullptr, nullptr};

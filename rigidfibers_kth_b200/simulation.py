@@ -256,6 +256,22 @@ class Simulation:
     def stream(self):
         return L.lib().rf_get_stream(self._h)
 
+    def mark(self, slot):
+        """Record device-time marker ``slot`` (0..15) on the handle's stream."""
+        L.check(L.lib().rf_timer_mark(self._h, slot), self._h)
+
+    def elapsed_ms(self, start, end):
+        ms = L.lib().rf_timer_elapsed_ms(self._h, start, end)
+        if ms < 0:
+            raise RuntimeError("timer slots not recorded")
+        return ms
+
+    def profile_matvec(self, reps=10):
+        """(ms per product, bytes of A per product) of the inner-solve matvec."""
+        ms, nbytes = ctypes.c_double(), ctypes.c_double()
+        L.check(L.lib().rf_profile_matvec(self._h, reps, ctypes.byref(ms), ctypes.byref(nbytes)), self._h)
+        return ms.value, nbytes.value
+
     def kernel_launches(self):
         return L.lib().rf_kernel_launches(self._h)
 
