@@ -148,6 +148,21 @@ rf_status rf_get_matrix(rf_handle *h, double *A);
 /* y = A x with the stored matrix (FP64 host vectors of n doubles). */
 rf_status rf_matvec(rf_handle *h, const double *x, double *y);
 rf_status rf_get_solve_stats(rf_handle *h, rf_solve_stats *s);
+/* y = A x in FP64 for callers that cannot allocate device memory: A (n x n
+ * column-major, leading dimension lda, lda*n doubles, 16-byte aligned), x and
+ * y are the caller's device buffers, and the product's partial sums use an
+ * 8 MiB array that the library reserves on every GPU that loads it, kept
+ * until the process exits.  No counterpart in the reference: it serves hosts
+ * whose device memory belongs to their own allocator or pool, and loops that
+ * must not stall on cudaMalloc/cudaFree.  Limit: lda <= 1,048,576 (lda even);
+ * larger sizes return RF_ERR_INVALID_ARG with the reason in
+ * rf_last_error(NULL).  Enqueued on `stream` (cudaStream_t, NULL = default
+ * stream) of the current device; y is ready when the stream reaches it.  The
+ * first call on a device looks up the array's device address, so make that
+ * call before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race on it.  Nothing in
+ * the array needs to start at zero. */
+rf_status rf_matvec_noalloc(const double *A, int64_t lda, int64_t n, const double *x, double *y, void *stream);
 /* Multistep history for checkpoint/resume: previous positions/orientations
  * and previous velocities (3*M doubles each). */
 rf_status rf_get_history(rf_handle *h, double *prev_pos, double *prev_orient, double *prev_vel,
