@@ -54,7 +54,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--M", type=int, default=WORKLOAD["M"], help="override the number of fibers (smoke runs)")
     ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
-    ap.add_argument("--pc", choices=["learned", "cluster", "none"], default="none")
+    ap.add_argument("--pc", choices=["learned", "cluster", "none"], default="learned")
     ap.add_argument("--weights", default=os.path.join(ROOT, "rigidfibers_kth_b200", "mlp_weights.npy"))
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

@@ -1,31 +1,795 @@
-// precond.cu - block preconditioners (filled in below).
+// precond.cu - block preconditioners for the right-preconditioned GMRES.
+//
+// The 3N x 3N diagonal blocks of A are the identity (matrix_assembly.f90:
+// 489-492), so plain block-Jacobi is no preconditioning at all.  The blocks
+// used here approximate the fiber's own block of the inverse instead:
+//
+//   RF_PC_CLUSTER  B_i = [S_i^-1]_00, S_i = A restricted to fiber i and its
+//                  k nearest neighbours (the "exact local-cluster block
+//                  inverse"); one CTA per fiber factorises S_i in shared
+//                  memory (FP32 LU with partial pivoting).
+//   RF_PC_LEARNED  B_i = I + R_i^T O_i R_i, O_i the output of a small MLP on
+//                  the geometry of the 16 nearest neighbours expressed in a
+//                  frame attached to fiber i (R_i = blockdiag of the frame
+//                  rotation).  The inverse blocks transform as
+//                  B(Q config) = Q B(config) Q^T under rotations Q, so the
+//                  network only learns the rotation-free part.
+//
+// The MLP (144 -> 256 -> 256 -> 225, ReLU) is trained by the trainer below
+// with hand-written FP32 GEMM kernels (forward and backward) and Adam.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
 #include "handle.h"
 
 namespace rf {
+namespace {
 
-rf_status build_preconditioner(rf_handle *h) {
-    return fail(h, RF_ERR_INVALID_ARG, "preconditioner not available");
+constexpr int kK = RF_MLP_K;          // neighbours in the features
+constexpr int kIn = RF_MLP_IN;        // 144
+constexpr int kHid = RF_MLP_HIDDEN;   // 256
+constexpr int kOut = RF_MLP_OUT;      // 225
+constexpr int kNb = 15;               // block size the MLP is built for (N = 5)
+
+// ------------------------------------------------------------------ k-NN
+// One thread per fiber: the K nearest centres (excluding itself), sorted.
+__global__ void knn_kernel(int M, const double *__restrict__ pos, int K, int *__restrict__ knn) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    float bd[16];
+    int bi[16];
+    for (int r = 0; r < 16; ++r) {
+        bd[r] = 3.4e38f;
+        bi[r] = -1;
+    }
+    const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+    for (int j = 0; j < M; ++j) {
+        if (j == i) continue;
+        const float dx = (float)(__ldg(pos + 3 * j) - xi), dy = (float)(__ldg(pos + 3 * j + 1) - yi),
+                    dz = (float)(__ldg(pos + 3 * j + 2) - zi);
+        const float d = dx * dx + dy * dy + dz * dz;
+        if (d >= bd[K - 1]) continue;
+        int r = K - 1;
+        while (r > 0 && bd[r - 1] > d) {
+            bd[r] = bd[r - 1];
+            bi[r] = bi[r - 1];
+            --r;
+        }
+        bd[r] = d;
+        bi[r] = j;
+    }
+    for (int r = 0; r < K; ++r) knn[(int64_t)i * K + r] = bi[r];
 }
 
-rf_status apply_mlp(rf_handle *h) { return fail(h, RF_ERR_INVALID_ARG, "MLP not available"); }
+// ------------------------------------------------------------------ cluster inverse
+// S = A[C, C] with C = {i, knn_0, .., knn_{kc-1}}; solve S X = E (E = the
+// first nb columns of the identity) by LU with partial pivoting in shared
+// memory and keep X[0:nb, 0:nb].
+template <typename T>
+__global__ void __launch_bounds__(256) cluster_inverse_kernel(int M, int nb, const T *__restrict__ A, int64_t lda,
+                                                              const int *__restrict__ knn, int K, int kc,
+                                                              float *__restrict__ out, int *__restrict__ singular) {
+    extern __shared__ float sm[];
+    __shared__ int s_fib[32];
+    __shared__ int s_piv;
+    __shared__ float s_pval;
+    const int i = blockIdx.x;
+    const int s = (kc + 1) * nb;
+    const int w = s + nb;       // augmented width
+    const int ld = w + 1;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid <= kc) s_fib[tid] = tid == 0 ? i : knn[(int64_t)i * K + tid - 1];
+    __syncthreads();
+    // gather the cluster matrix (column-major in A: consecutive threads read
+    // consecutive rows of one column)
+    for (int idx = tid; idx < s * s; idx += nt) {
+        const int c = idx / s, r = idx - c * s;
+        const int64_t gr = (int64_t)s_fib[r / nb] * nb + r % nb;
+        const int64_t gc = (int64_t)s_fib[c / nb] * nb + c % nb;
+        sm[r * ld + c] = (float)A[gc * lda + gr];
+    }
+    for (int idx = tid; idx < s * nb; idx += nt) {
+        const int r = idx / nb, j = idx - r * nb;
+        sm[r * ld + s + j] = (r == j) ? 1.f : 0.f;
+    }
+    __syncthreads();
+    bool bad = false;
+    for (int k = 0; k < s; ++k) {
+        // pivot: warp 0 finds the largest |S[r][k]|, r >= k
+        if (tid < 32) {
+            float best = -1.f;
+            int br = k;
+            for (int r = k + tid; r < s; r += 32) {
+                const float v = fabsf(sm[r * ld + k]);
+                if (v > best) {
+                    best = v;
+                    br = r;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int orow = __shfl_xor_sync(0xffffffffu, br, o);
+                if (ob > best || (ob == best && orow < br)) {
+                    best = ob;
+                    br = orow;
+                }
+            }
+            if (tid == 0) {
+                s_piv = br;
+                s_pval = best;
+            }
+        }
+        __syncthreads();
+        if (!(s_pval > 0.f)) {
+            bad = true;
+            break;
+        }
+        const int p = s_piv;
+        if (p != k)
+            for (int c = k + tid; c < w; c += nt) {
+                const float t = sm[k * ld + c];
+                sm[k * ld + c] = sm[p * ld + c];
+                sm[p * ld + c] = t;
+            }
+        __syncthreads();
+        const float inv = 1.f / sm[k * ld + k];
+        for (int r = k + 1 + tid; r < s; r += nt) sm[r * ld + k] *= inv;
+        __syncthreads();
+        const int rows = s - k - 1, cols = w - k - 1;
+        for (int idx = tid; idx < rows * cols; idx += nt) {
+            const int rr = idx / cols, cc = idx - rr * cols;
+            const int r = k + 1 + rr, c = k + 1 + cc;
+            sm[r * ld + c] -= sm[r * ld + k] * sm[k * ld + c];
+        }
+        __syncthreads();
+    }
+    if (bad) {
+        if (tid == 0) atomicAdd(singular, 1);
+        for (int idx = tid; idx < nb * nb; idx += nt)
+            out[(int64_t)i * nb * nb + idx] = (idx / nb == idx % nb) ? 1.f : 0.f;
+        return;
+    }
+    // back substitution on the nb right-hand sides, column-oriented: x_k,
+    // then remove its contribution from the rows above
+    for (int k = s - 1; k >= 0; --k) {
+        if (tid < nb) sm[k * ld + s + tid] /= sm[k * ld + k];
+        __syncthreads();
+        for (int idx = tid; idx < k * nb; idx += nt) {
+            const int r = idx / nb, j = idx - r * nb;
+            sm[r * ld + s + j] -= sm[r * ld + k] * sm[k * ld + s + j];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < nb * nb; idx += nt) {
+        const int a = idx / nb, b = idx - a * nb;
+        out[(int64_t)i * nb * nb + idx] = sm[a * ld + s + b];
+    }
+}
+
+// ------------------------------------------------------------------ features
+// Frame of fiber i: e3 = t_i, e1 = the direction to the nearest neighbour
+// with its t_i component removed, e2 = e3 x e1.  Per neighbour (nearest
+// first): its centre relative to x_i in that frame, and the six distinct
+// products u_a u_b of its orientation u in the frame (invariant under the
+// sign of u, like the inverse block itself).
+__global__ void features_kernel(int M, const double *__restrict__ pos, const double *__restrict__ ori,
+                                const int *__restrict__ knn, float *__restrict__ feat, float *__restrict__ rot) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    const double *xi = pos + 3 * i, *ti = ori + 3 * i;
+    double e3[3] = {ti[0], ti[1], ti[2]};
+    const int j0 = knn[(int64_t)i * kK];
+    double d1[3] = {pos[3 * j0] - xi[0], pos[3 * j0 + 1] - xi[1], pos[3 * j0 + 2] - xi[2]};
+    double dot = d1[0] * e3[0] + d1[1] * e3[1] + d1[2] * e3[2];
+    double e1[3] = {d1[0] - dot * e3[0], d1[1] - dot * e3[1], d1[2] - dot * e3[2]};
+    double n1 = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    if (n1 < 1e-9) {  // neighbour on the axis: any perpendicular direction
+        const double a[3] = {fabs(e3[0]) < 0.9 ? 1.0 : 0.0, fabs(e3[0]) < 0.9 ? 0.0 : 1.0, 0.0};
+        dot = a[0] * e3[0] + a[1] * e3[1];
+        e1[0] = a[0] - dot * e3[0];
+        e1[1] = a[1] - dot * e3[1];
+        e1[2] = -dot * e3[2];
+        n1 = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    }
+    for (int a = 0; a < 3; ++a) e1[a] /= n1;
+    const double e2[3] = {e3[1] * e1[2] - e3[2] * e1[1], e3[2] * e1[0] - e3[0] * e1[2], e3[0] * e1[1] - e3[1] * e1[0]};
+    const double *E[3] = {e1, e2, e3};
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) rot[(int64_t)i * 9 + r * 3 + c] = (float)E[r][c];
+    float *f = feat + (int64_t)i * kIn;
+    for (int n = 0; n < kK; ++n) {
+        const int j = knn[(int64_t)i * kK + n];
+        const double d[3] = {pos[3 * j] - xi[0], pos[3 * j + 1] - xi[1], pos[3 * j + 2] - xi[2]};
+        const double *tj = ori + 3 * j;
+        double dl[3], ul[3];
+        for (int r = 0; r < 3; ++r) {
+            dl[r] = E[r][0] * d[0] + E[r][1] * d[1] + E[r][2] * d[2];
+            ul[r] = E[r][0] * tj[0] + E[r][1] * tj[1] + E[r][2] * tj[2];
+        }
+        float *g = f + n * 9;
+        g[0] = (float)dl[0];
+        g[1] = (float)dl[1];
+        g[2] = (float)dl[2];
+        g[3] = (float)(ul[0] * ul[0]);
+        g[4] = (float)(ul[1] * ul[1]);
+        g[5] = (float)(ul[2] * ul[2]);
+        g[6] = (float)(ul[0] * ul[1]);
+        g[7] = (float)(ul[0] * ul[2]);
+        g[8] = (float)(ul[1] * ul[2]);
+    }
+}
+
+// local <-> global block transform: B = I + R_blk^T O R_blk (to_global) or
+// O = R_blk (B - I) R_blk^T (to_local), R_blk = I_5 (x) R, per fiber.
+__global__ void block_frame_kernel(int M, const float *__restrict__ rot, const float *__restrict__ in,
+                                   float *__restrict__ out, int to_global) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    float R[9];
+    for (int t = 0; t < 9; ++t) R[t] = rot[(int64_t)i * 9 + t];
+    const float *X = in + (int64_t)i * kOut;
+    float *Y = out + (int64_t)i * kOut;
+    for (int kb = 0; kb < 5; ++kb)
+        for (int lb = 0; lb < 5; ++lb) {
+            float O[3][3], T[3][3], Z[3][3];
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    float v = X[(kb * 3 + a) * kNb + lb * 3 + b];
+                    if (!to_global && kb == lb && a == b) v -= 1.f;
+                    O[a][b] = v;
+                }
+            // to_global: Z = R^T O R ; to_local: Z = R O R^T
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    float sacc = 0.f;
+                    for (int c = 0; c < 3; ++c) sacc += O[a][c] * (to_global ? R[c * 3 + b] : R[b * 3 + c]);
+                    T[a][b] = sacc;
+                }
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                    float sacc = 0.f;
+                    for (int c = 0; c < 3; ++c) sacc += (to_global ? R[c * 3 + a] : R[a * 3 + c]) * T[c][b];
+                    Z[a][b] = sacc;
+                }
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    Y[(kb * 3 + a) * kNb + lb * 3 + b] = Z[a][b] + ((to_global && kb == lb && a == b) ? 1.f : 0.f);
+        }
+}
+
+// ------------------------------------------------------------------ FP32 GEMM
+// C[i][j] = act( alpha * sum_k A(i,k) B(k,j) + bias[j] ) (+ beta C), generic
+// strides so one kernel serves X W^T, dY W and dY^T X.  64x64 tiles, 16-deep,
+// 256 threads with 4x4 outputs each.
+struct GemmArgs {
+    int m, n, k;
+    const float *A;
+    int64_t sai, sak;
+    const float *B;
+    int64_t sbk, sbj;
+    float *C;
+    int64_t ldc;
+    const float *bias;
+    int relu;
+    float beta;
+};
+
+__global__ void __launch_bounds__(256) gemm_kernel(GemmArgs g) {
+    __shared__ float As[16][64 + 4];
+    __shared__ float Bs[16][64 + 4];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < g.k; k0 += 16) {
+        for (int t = threadIdx.x; t < 16 * 64; t += 256) {
+            const int kk = t / 64, r = t % 64;
+            const int gi = i0 + r, gk = k0 + kk;
+            As[kk][r] = (gi < g.m && gk < g.k) ? g.A[gi * g.sai + gk * g.sak] : 0.f;
+            const int gj = j0 + r;
+            Bs[kk][r] = (gj < g.n && gk < g.k) ? g.B[gk * g.sbk + gj * g.sbj] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u] = As[kk][ty * 4 + u];
+                b[u] = Bs[kk][tx * 4 + u];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+            if (i >= g.m || j >= g.n) continue;
+            float val = acc[u][v];
+            if (g.bias) val += g.bias[j];
+            if (g.relu) val = fmaxf(val, 0.f);
+            float *c = g.C + (int64_t)i * g.ldc + j;
+            *c = g.beta != 0.f ? g.beta * *c + val : val;
+        }
+}
+
+cudaError_t gemm(const GemmArgs &g, cudaStream_t st) {
+    dim3 grid((g.n + 63) / 64, (g.m + 63) / 64);
+    gemm_kernel<<<grid, 256, 0, st>>>(g);
+    return cudaGetLastError();
+}
+
+// column sums of an m x n row-major matrix (bias gradients)
+__global__ void colsum_kernel(int m, int n, const float *__restrict__ X, float *__restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float s = 0.f;
+    for (int i = 0; i < m; ++i) s += X[(int64_t)i * n + j];
+    out[j] = s;
+}
+
+// dY = 2 (Y - T) / count, and per-block partial sums of (Y - T)^2
+__global__ void mse_grad_kernel(int64_t cnt, const float *__restrict__ Y, const float *__restrict__ T,
+                                float *__restrict__ dY, double *__restrict__ part) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        const float d = Y[e] - T[e];
+        dY[e] = 2.f * d / (float)cnt;
+        acc += (double)d * d;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void relu_back_kernel(int64_t cnt, const float *__restrict__ H, float *__restrict__ dH) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x)
+        if (H[e] <= 0.f) dH[e] = 0.f;
+}
+
+__global__ void adam_kernel(int64_t cnt, float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, float lr, float b1, float b2, float c1, float c2, float eps) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+        const float gi = g[e];
+        const float mi = b1 * m[e] + (1.f - b1) * gi;
+        const float vi = b2 * v[e] + (1.f - b2) * gi * gi;
+        m[e] = mi;
+        v[e] = vi;
+        w[e] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void gather_rows_kernel(int rows, int width, const int *__restrict__ idx, const float *__restrict__ src,
+                                   float *__restrict__ dst) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (int64_t)rows * width) return;
+    const int r = (int)(e / width), c = (int)(e - (int64_t)r * width);
+    dst[e] = src[(int64_t)idx[r] * width + c];
+}
+
+// parameter offsets inside the packed weight vector
+struct MlpLayout {
+    int64_t w1 = 0, b1 = w1 + (int64_t)kHid * kIn, w2 = b1 + kHid, b2 = w2 + (int64_t)kHid * kHid, w3 = b2 + kHid,
+            b3 = w3 + (int64_t)kOut * kHid, total = b3 + kOut;
+};
+
+// Forward pass for `rows` samples: H1, H2, O (row-major)
+cudaError_t mlp_forward(const float *W, int rows, const float *X, float *H1, float *H2, float *O, cudaStream_t st) {
+    const MlpLayout L;
+    GemmArgs g{};
+    g.m = rows; g.n = kHid; g.k = kIn;
+    g.A = X; g.sai = kIn; g.sak = 1;
+    g.B = W + L.w1; g.sbk = 1; g.sbj = kIn;           // B(k,j) = W1[j][k]
+    g.C = H1; g.ldc = kHid; g.bias = W + L.b1; g.relu = 1;
+    cudaError_t e = gemm(g, st);
+    if (e != cudaSuccess) return e;
+    g.k = kHid; g.A = H1; g.sai = kHid; g.B = W + L.w2; g.sbj = kHid; g.C = H2; g.bias = W + L.b2;
+    e = gemm(g, st);
+    if (e != cudaSuccess) return e;
+    g.n = kOut; g.A = H2; g.B = W + L.w3; g.sbj = kHid; g.C = O; g.ldc = kOut; g.bias = W + L.b3; g.relu = 0;
+    return gemm(g, st);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ handle side
+rf_status build_preconditioner(rf_handle *h) {
+    const int M = h->M, nb = 3 * h->N;
+    cudaStream_t st = h->stream;
+    auto ck = [&](cudaError_t e, const char *what) -> rf_status {
+        return e == cudaSuccess ? RF_OK : cuda_fail(h, e, what);
+    };
+    rf_status s;
+    if (!h->Pblocks) {
+        if ((s = ck(cudaMalloc(&h->Pblocks, sizeof(float) * (size_t)M * nb * nb), "alloc blocks")) != RF_OK) return s;
+    }
+    const int kmax = kK;
+    if (!h->knn) {
+        if ((s = ck(cudaMalloc(&h->knn, sizeof(int) * (size_t)M * kmax), "alloc knn")) != RF_OK) return s;
+    }
+    const int K = std::min(kmax, M - 1);
+    knn_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, h->X[h->cur], K, h->knn);
+    h->launches++;
+    if ((s = ck(cudaGetLastError(), "knn")) != RF_OK) return s;
+    if (h->p.preconditioner == RF_PC_CLUSTER) {
+        const int kc = std::min(h->p.cluster_size, K);
+        const int sdim = (kc + 1) * nb;
+        const size_t smem = sizeof(float) * (size_t)sdim * (sdim + nb + 1);
+        if (smem > 227 * 1024)
+            return fail(h, RF_ERR_INVALID_ARG, "cluster_size too large for the shared-memory factorisation");
+        int *sing = nullptr;
+        if ((s = ck(cudaMalloc(&sing, sizeof(int)), "alloc")) != RF_OK) return s;
+        cudaMemsetAsync(sing, 0, sizeof(int), st);
+        cudaError_t e;
+        if (h->A64) {
+            e = cudaFuncSetAttribute(cluster_inverse_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            if (e == cudaSuccess)
+                cluster_inverse_kernel<double><<<M, 256, smem, st>>>(M, nb, h->A64, h->lda, h->knn, K, kc, h->Pblocks,
+                                                                     sing);
+        } else {
+            e = cudaFuncSetAttribute(cluster_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            if (e == cudaSuccess)
+                cluster_inverse_kernel<float><<<M, 256, smem, st>>>(M, nb, h->A32, h->lda, h->knn, K, kc, h->Pblocks,
+                                                                    sing);
+        }
+        h->launches++;
+        if (e == cudaSuccess) e = cudaGetLastError();
+        cudaFree(sing);
+        if ((s = ck(e, "cluster inverse")) != RF_OK) return s;
+        h->pc_ready = true;
+        return RF_OK;
+    }
+    // learned
+    if (!h->mlp_loaded || nb != kNb || K < kK) {
+        h->pc_ready = false;  // fallback: no preconditioning (block-Jacobi with identity blocks)
+        return RF_OK;
+    }
+    return apply_mlp(h);
+}
+
+rf_status apply_mlp(rf_handle *h) {
+    const int M = h->M;
+    cudaStream_t st = h->stream;
+    auto ck = [&](cudaError_t e, const char *what) -> rf_status {
+        return e == cudaSuccess ? RF_OK : cuda_fail(h, e, what);
+    };
+    rf_status s;
+    if (!h->feat) {
+        if ((s = ck(cudaMalloc(&h->feat, sizeof(float) * ((size_t)M * (kIn + 9))), "alloc")) != RF_OK) return s;
+        if ((s = ck(cudaMalloc(&h->mlp_h1, sizeof(float) * (size_t)M * kHid), "alloc")) != RF_OK) return s;
+        if ((s = ck(cudaMalloc(&h->mlp_h2, sizeof(float) * (size_t)M * kHid), "alloc")) != RF_OK) return s;
+        if ((s = ck(cudaMalloc(&h->mlp_out, sizeof(float) * (size_t)M * kOut), "alloc")) != RF_OK) return s;
+    }
+    float *rot = h->feat + (size_t)M * kIn;
+    features_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, h->X[h->cur], h->T[h->cur], h->knn, h->feat, rot);
+    if ((s = ck(cudaGetLastError(), "features")) != RF_OK) return s;
+    if ((s = ck(mlp_forward(h->mlp_w, M, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out, st), "mlp")) != RF_OK) return s;
+    block_frame_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, rot, h->mlp_out, h->Pblocks, 1);
+    h->launches += 5;
+    if ((s = ck(cudaGetLastError(), "block frame")) != RF_OK) return s;
+    h->pc_ready = true;
+    return RF_OK;
+}
 
 }  // namespace rf
 
+// ------------------------------------------------------------------ C ABI
+using namespace rf;
+
+struct rf_trainer {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    float *W = nullptr, *G = nullptr, *Mom = nullptr, *Var = nullptr;
+    float *X = nullptr, *Y = nullptr;      // dataset
+    int64_t count = 0, cap = 0;
+    float *bx = nullptr, *by = nullptr, *h1 = nullptr, *h2 = nullptr, *o = nullptr, *dO = nullptr, *dh2 = nullptr,
+          *dh1 = nullptr;
+    int *bidx = nullptr;
+    int bcap = 0;
+    double *part = nullptr;
+    int64_t t = 0;
+    std::mt19937_64 rng;
+};
+
 extern "C" {
-int64_t rf_mlp_num_params(void) {
-    return (int64_t)RF_MLP_HIDDEN * RF_MLP_IN + RF_MLP_HIDDEN + (int64_t)RF_MLP_HIDDEN * RF_MLP_HIDDEN +
-           RF_MLP_HIDDEN + (int64_t)RF_MLP_OUT * RF_MLP_HIDDEN + RF_MLP_OUT;
+
+int64_t rf_mlp_num_params(void) { return MlpLayout().total; }
+
+rf_status rf_set_mlp_weights(rf_handle *h, const float *weights, int64_t count) {
+    if (!h || !weights || count != MlpLayout().total) return fail(h, RF_ERR_INVALID_ARG, "weights: wrong size");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, RF_ERR_CUDA, "cudaSetDevice");
+    if (!h->mlp_w && cudaMalloc(&h->mlp_w, sizeof(float) * count) != cudaSuccess)
+        return fail(h, RF_ERR_OOM, "alloc weights");
+    if (cudaMemcpy(h->mlp_w, weights, sizeof(float) * count, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(h, RF_ERR_CUDA, "upload weights");
+    h->mlp_loaded = true;
+    h->pc_ready = false;
+    return RF_OK;
 }
-rf_status rf_set_mlp_weights(rf_handle *h, const float *, int64_t) { return rf::fail(h, RF_ERR_INVALID_ARG, "n/a"); }
-rf_status rf_compute_features(rf_handle *h, float *) { return rf::fail(h, RF_ERR_INVALID_ARG, "n/a"); }
-rf_status rf_compute_cluster_targets(rf_handle *h, float *) { return rf::fail(h, RF_ERR_INVALID_ARG, "n/a"); }
-rf_status rf_trainer_create(int32_t, uint64_t, rf_trainer **) { return RF_ERR_INVALID_ARG; }
-rf_status rf_trainer_destroy(rf_trainer *) { return RF_ERR_INVALID_ARG; }
-rf_status rf_trainer_add_samples(rf_trainer *, const float *, const float *, int64_t) { return RF_ERR_INVALID_ARG; }
-rf_status rf_trainer_train(rf_trainer *, int32_t, int32_t, float, float *) { return RF_ERR_INVALID_ARG; }
-rf_status rf_trainer_get_weights(rf_trainer *, float *) { return RF_ERR_INVALID_ARG; }
-rf_status rf_trainer_set_weights(rf_trainer *, const float *) { return RF_ERR_INVALID_ARG; }
-rf_status rf_trainer_loss_grad(rf_trainer *, const float *, const float *, int64_t, float *, float *) {
-    return RF_ERR_INVALID_ARG;
+
+rf_status rf_compute_features(rf_handle *h, float *features) {
+    if (!h || !features) return fail(h, RF_ERR_INVALID_ARG, "null argument");
+    if (h->M <= kK) return fail(h, RF_ERR_INVALID_ARG, "features need more than 16 fibers");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, RF_ERR_CUDA, "cudaSetDevice");
+    const int M = h->M;
+    if (!h->knn && cudaMalloc(&h->knn, sizeof(int) * (size_t)M * kK) != cudaSuccess) return fail(h, RF_ERR_OOM, "alloc");
+    if (!h->feat) {
+        if (cudaMalloc(&h->feat, sizeof(float) * ((size_t)M * (kIn + 9))) != cudaSuccess ||
+            cudaMalloc(&h->mlp_h1, sizeof(float) * (size_t)M * kHid) != cudaSuccess ||
+            cudaMalloc(&h->mlp_h2, sizeof(float) * (size_t)M * kHid) != cudaSuccess ||
+            cudaMalloc(&h->mlp_out, sizeof(float) * (size_t)M * kOut) != cudaSuccess)
+            return fail(h, RF_ERR_OOM, "alloc");
+    }
+    knn_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->X[h->cur], kK, h->knn);
+    features_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->X[h->cur], h->T[h->cur], h->knn, h->feat,
+                                                            h->feat + (size_t)M * kIn);
+    h->launches += 2;
+    cudaError_t e = cudaMemcpyAsync(features, h->feat, sizeof(float) * (size_t)M * kIn, cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "features");
+    return RF_OK;
 }
+
+rf_status rf_compute_cluster_targets(rf_handle *h, float *targets) {
+    if (!h || !targets) return fail(h, RF_ERR_INVALID_ARG, "null argument");
+    if (!h->assembled) return fail(h, RF_ERR_INVALID_ARG, "cluster targets need an assembled system");
+    if (3 * h->N != kNb) return fail(h, RF_ERR_INVALID_ARG, "the learned blocks are built for N = 5");
+    if (h->M <= kK) return fail(h, RF_ERR_INVALID_ARG, "targets need more than 16 fibers");
+    if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, RF_ERR_CUDA, "cudaSetDevice");
+    const int saved = h->p.preconditioner;
+    h->p.preconditioner = RF_PC_CLUSTER;
+    rf_status s = build_preconditioner(h);   // exact blocks into Pblocks
+    h->p.preconditioner = saved;
+    if (s != RF_OK) return s;
+    const int M = h->M;
+    // features (frames) of the same state, then the blocks in that frame minus I
+    std::vector<float> tmp((size_t)M * kIn);
+    s = rf_compute_features(h, tmp.data());
+    if (s != RF_OK) return s;
+    block_frame_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->feat + (size_t)M * kIn, h->Pblocks, h->mlp_out, 0);
+    h->launches++;
+    cudaError_t e = cudaMemcpyAsync(targets, h->mlp_out, sizeof(float) * (size_t)M * kOut, cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "targets");
+    if (saved != RF_PC_CLUSTER) h->pc_ready = false;
+    return RF_OK;
 }
+
+rf_status rf_trainer_create(int32_t device, uint64_t seed, rf_trainer **out) {
+    if (!out) return fail(nullptr, RF_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, RF_ERR_NO_DEVICE, "no CUDA device");
+    }
+    rf_trainer *t = new rf_trainer;
+    t->device = device;
+    t->rng.seed(seed);
+    const int64_t P = MlpLayout().total;
+    bool ok = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(&t->W, sizeof(float) * P) == cudaSuccess && cudaMalloc(&t->G, sizeof(float) * P) == cudaSuccess &&
+              cudaMalloc(&t->Mom, sizeof(float) * P) == cudaSuccess && cudaMalloc(&t->Var, sizeof(float) * P) == cudaSuccess &&
+              cudaMalloc(&t->part, sizeof(double) * 1024) == cudaSuccess;
+    if (!ok) {
+        rf_trainer_destroy(t);
+        return fail(nullptr, RF_ERR_OOM, "trainer allocation");
+    }
+    // He-uniform initial weights, small output layer, zero biases
+    const MlpLayout L;
+    std::vector<float> w(P, 0.f);
+    auto fill = [&](int64_t off, int fan_out, int fan_in, float gain) {
+        std::uniform_real_distribution<float> u(-1.f, 1.f);
+        const float a = gain * std::sqrt(6.f / fan_in);
+        for (int64_t e = 0; e < (int64_t)fan_out * fan_in; ++e) w[off + e] = a * u(t->rng);
+    };
+    fill(L.w1, kHid, kIn, 1.f);
+    fill(L.w2, kHid, kHid, 1.f);
+    fill(L.w3, kOut, kHid, 0.1f);
+    cudaMemcpy(t->W, w.data(), sizeof(float) * P, cudaMemcpyHostToDevice);
+    cudaMemset(t->Mom, 0, sizeof(float) * P);
+    cudaMemset(t->Var, 0, sizeof(float) * P);
+    *out = t;
+    return RF_OK;
+}
+
+rf_status rf_trainer_destroy(rf_trainer *t) {
+    if (!t) return RF_ERR_INVALID_ARG;
+    cudaSetDevice(t->device);
+    void *ptrs[] = {t->W, t->G, t->Mom, t->Var, t->X, t->Y, t->bx, t->by, t->h1, t->h2, t->o, t->dO, t->dh2, t->dh1,
+                    t->bidx, t->part};
+    for (void *p : ptrs) cudaFree(p);
+    if (t->stream) cudaStreamDestroy(t->stream);
+    delete t;
+    return RF_OK;
+}
+
+rf_status rf_trainer_add_samples(rf_trainer *t, const float *features, const float *targets, int64_t count) {
+    if (!t || !features || !targets || count < 1) return fail(nullptr, RF_ERR_INVALID_ARG, "bad samples");
+    cudaSetDevice(t->device);
+    if (t->count + count > t->cap) {
+        int64_t ncap = std::max<int64_t>(t->cap * 2, t->count + count);
+        float *nx = nullptr, *ny = nullptr;
+        if (cudaMalloc(&nx, sizeof(float) * ncap * kIn) != cudaSuccess ||
+            cudaMalloc(&ny, sizeof(float) * ncap * kOut) != cudaSuccess) {
+            cudaFree(nx);
+            return fail(nullptr, RF_ERR_OOM, "dataset");
+        }
+        if (t->count) {
+            cudaMemcpy(nx, t->X, sizeof(float) * t->count * kIn, cudaMemcpyDeviceToDevice);
+            cudaMemcpy(ny, t->Y, sizeof(float) * t->count * kOut, cudaMemcpyDeviceToDevice);
+        }
+        cudaFree(t->X);
+        cudaFree(t->Y);
+        t->X = nx;
+        t->Y = ny;
+        t->cap = ncap;
+    }
+    if (cudaMemcpy(t->X + t->count * kIn, features, sizeof(float) * count * kIn, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(t->Y + t->count * kOut, targets, sizeof(float) * count * kOut, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(nullptr, RF_ERR_CUDA, "upload samples");
+    t->count += count;
+    return RF_OK;
+}
+
+namespace {
+bool ensure_batch(rf_trainer *t, int B) {
+    if (B <= t->bcap) return true;
+    void *ptrs[] = {t->bx, t->by, t->h1, t->h2, t->o, t->dO, t->dh2, t->dh1, t->bidx};
+    for (void *p : ptrs) cudaFree(p);
+    bool ok = cudaMalloc(&t->bx, sizeof(float) * B * kIn) == cudaSuccess &&
+              cudaMalloc(&t->by, sizeof(float) * B * kOut) == cudaSuccess &&
+              cudaMalloc(&t->h1, sizeof(float) * B * kHid) == cudaSuccess &&
+              cudaMalloc(&t->h2, sizeof(float) * B * kHid) == cudaSuccess &&
+              cudaMalloc(&t->o, sizeof(float) * B * kOut) == cudaSuccess &&
+              cudaMalloc(&t->dO, sizeof(float) * B * kOut) == cudaSuccess &&
+              cudaMalloc(&t->dh2, sizeof(float) * B * kHid) == cudaSuccess &&
+              cudaMalloc(&t->dh1, sizeof(float) * B * kHid) == cudaSuccess &&
+              cudaMalloc(&t->bidx, sizeof(int) * B) == cudaSuccess;
+    t->bcap = ok ? B : 0;
+    return ok;
+}
+
+// forward + backward on B samples already in bx/by; gradient into G; returns
+// the summed squared error (over B*225 outputs)
+cudaError_t forward_backward(rf_trainer *t, int B, double *sse) {
+    const MlpLayout L;
+    cudaStream_t st = t->stream;
+    cudaError_t e = mlp_forward(t->W, B, t->bx, t->h1, t->h2, t->o, st);
+    if (e != cudaSuccess) return e;
+    const int64_t cnt = (int64_t)B * kOut;
+    const int nblk = (int)std::min<int64_t>(1024, (cnt + 255) / 256);
+    mse_grad_kernel<<<nblk, 256, 0, st>>>(cnt, t->o, t->by, t->dO, t->part);
+    // layer 3: dW3 = dO^T H2, db3 = colsum dO, dH2 = dO W3 (relu mask)
+    GemmArgs g{};
+    g.m = kOut; g.n = kHid; g.k = B;
+    g.A = t->dO; g.sai = 1; g.sak = kOut;           // A(i,k) = dO[k][i]
+    g.B = t->h2; g.sbk = kHid; g.sbj = 1;
+    g.C = t->G + L.w3; g.ldc = kHid;
+    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    colsum_kernel<<<(kOut + 255) / 256, 256, 0, st>>>(B, kOut, t->dO, t->G + L.b3);
+    g = GemmArgs{};
+    g.m = B; g.n = kHid; g.k = kOut;
+    g.A = t->dO; g.sai = kOut; g.sak = 1;
+    g.B = t->W + L.w3; g.sbk = kHid; g.sbj = 1;     // B(k,j) = W3[k][j]
+    g.C = t->dh2; g.ldc = kHid;
+    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    relu_back_kernel<<<256, 256, 0, st>>>((int64_t)B * kHid, t->h2, t->dh2);
+    // layer 2
+    g = GemmArgs{};
+    g.m = kHid; g.n = kHid; g.k = B;
+    g.A = t->dh2; g.sai = 1; g.sak = kHid;
+    g.B = t->h1; g.sbk = kHid; g.sbj = 1;
+    g.C = t->G + L.w2; g.ldc = kHid;
+    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    colsum_kernel<<<1, 256, 0, st>>>(B, kHid, t->dh2, t->G + L.b2);
+    g = GemmArgs{};
+    g.m = B; g.n = kHid; g.k = kHid;
+    g.A = t->dh2; g.sai = kHid; g.sak = 1;
+    g.B = t->W + L.w2; g.sbk = kHid; g.sbj = 1;
+    g.C = t->dh1; g.ldc = kHid;
+    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    relu_back_kernel<<<256, 256, 0, st>>>((int64_t)B * kHid, t->h1, t->dh1);
+    // layer 1
+    g = GemmArgs{};
+    g.m = kHid; g.n = kIn; g.k = B;
+    g.A = t->dh1; g.sai = 1; g.sak = kHid;
+    g.B = t->bx; g.sbk = kIn; g.sbj = 1;
+    g.C = t->G + L.w1; g.ldc = kIn;
+    if ((e = gemm(g, st)) != cudaSuccess) return e;
+    colsum_kernel<<<1, 256, 0, st>>>(B, kHid, t->dh1, t->G + L.b1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    std::vector<double> part(nblk);
+    e = cudaMemcpyAsync(part.data(), t->part, sizeof(double) * nblk, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    double s = 0.0;
+    for (double v : part) s += v;
+    *sse = s;
+    return e;
+}
+}  // namespace
+
+rf_status rf_trainer_train(rf_trainer *t, int32_t epochs, int32_t batch, float lr, float *loss) {
+    if (!t || epochs < 1 || batch < 1 || t->count < 1) return fail(nullptr, RF_ERR_INVALID_ARG, "bad training call");
+    cudaSetDevice(t->device);
+    if (!ensure_batch(t, batch)) return fail(nullptr, RF_ERR_OOM, "batch buffers");
+    const int64_t P = MlpLayout().total;
+    std::vector<int> perm(t->count);
+    double last = 0.0;
+    for (int ep = 0; ep < epochs; ++ep) {
+        for (int64_t i = 0; i < t->count; ++i) perm[i] = (int)i;
+        std::shuffle(perm.begin(), perm.end(), t->rng);
+        double sse = 0.0;
+        for (int64_t b0 = 0; b0 < t->count; b0 += batch) {
+            const int B = (int)std::min<int64_t>(batch, t->count - b0);
+            cudaMemcpyAsync(t->bidx, perm.data() + b0, sizeof(int) * B, cudaMemcpyHostToDevice, t->stream);
+            gather_rows_kernel<<<(unsigned)(((int64_t)B * kIn + 255) / 256), 256, 0, t->stream>>>(B, kIn, t->bidx, t->X,
+                                                                                                  t->bx);
+            gather_rows_kernel<<<(unsigned)(((int64_t)B * kOut + 255) / 256), 256, 0, t->stream>>>(B, kOut, t->bidx,
+                                                                                                   t->Y, t->by);
+            double s = 0.0;
+            cudaError_t e = forward_backward(t, B, &s);
+            if (e != cudaSuccess) return cuda_fail(nullptr, e, "training step");
+            sse += s;
+            t->t += 1;
+            const float b1 = 0.9f, b2 = 0.999f;
+            const float c1 = 1.f - std::pow(b1, (float)t->t), c2 = 1.f - std::pow(b2, (float)t->t);
+            adam_kernel<<<256, 256, 0, t->stream>>>(P, t->W, t->G, t->Mom, t->Var, lr, b1, b2, c1, c2, 1e-8f);
+        }
+        last = sse / ((double)t->count * kOut);
+    }
+    if (cudaStreamSynchronize(t->stream) != cudaSuccess) return fail(nullptr, RF_ERR_CUDA, "training");
+    if (loss) *loss = (float)last;
+    return RF_OK;
+}
+
+rf_status rf_trainer_get_weights(rf_trainer *t, float *weights) {
+    if (!t || !weights) return fail(nullptr, RF_ERR_INVALID_ARG, "null argument");
+    cudaSetDevice(t->device);
+    if (cudaMemcpy(weights, t->W, sizeof(float) * MlpLayout().total, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail(nullptr, RF_ERR_CUDA, "download weights");
+    return RF_OK;
+}
+
+rf_status rf_trainer_set_weights(rf_trainer *t, const float *weights) {
+    if (!t || !weights) return fail(nullptr, RF_ERR_INVALID_ARG, "null argument");
+    cudaSetDevice(t->device);
+    if (cudaMemcpy(t->W, weights, sizeof(float) * MlpLayout().total, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(nullptr, RF_ERR_CUDA, "upload weights");
+    return RF_OK;
+}
+
+rf_status rf_trainer_loss_grad(rf_trainer *t, const float *features, const float *targets, int64_t count, float *loss,
+                               float *grad) {
+    if (!t || !features || !targets || count < 1 || count > (1 << 20))
+        return fail(nullptr, RF_ERR_INVALID_ARG, "bad arguments");
+    cudaSetDevice(t->device);
+    if (!ensure_batch(t, (int)count)) return fail(nullptr, RF_ERR_OOM, "batch buffers");
+    cudaMemcpy(t->bx, features, sizeof(float) * count * kIn, cudaMemcpyHostToDevice);
+    cudaMemcpy(t->by, targets, sizeof(float) * count * kOut, cudaMemcpyHostToDevice);
+    double sse = 0.0;
+    cudaError_t e = forward_backward(t, (int)count, &sse);
+    if (e == cudaSuccess && grad)
+        e = cudaMemcpy(grad, t->G, sizeof(float) * MlpLayout().total, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "loss/grad");
+    if (loss) *loss = (float)(sse / ((double)count * kOut));
+    return RF_OK;
+}
+
+}  // extern "C"

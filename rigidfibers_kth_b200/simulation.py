@@ -266,6 +266,25 @@ class Simulation:
             raise RuntimeError("timer slots not recorded")
         return ms
 
+    # -- learned / cluster preconditioner -------------------------------------
+    def set_mlp_weights(self, weights):
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.check(L.lib().rf_set_mlp_weights(self._h, w.ctypes.data_as(fp), w.size), self._h)
+
+    def features(self):
+        """k-NN features (M x 144) of the current state in each fiber's frame."""
+        f = np.zeros((self.M, 144), dtype=np.float32)
+        L.check(L.lib().rf_compute_features(self._h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self._h)
+        return f
+
+    def cluster_targets(self):
+        """Exact cluster block inverses minus I, in each fiber's frame (M x 225); needs an assembled system."""
+        t = np.zeros((self.M, 225), dtype=np.float32)
+        L.check(L.lib().rf_compute_cluster_targets(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+                self._h)
+        return t
+
     def profile_matvec(self, reps=10):
         """(ms per product, bytes of A per product) of the inner-solve matvec."""
         ms, nbytes = ctypes.c_double(), ctypes.c_double()
