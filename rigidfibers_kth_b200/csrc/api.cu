@@ -33,7 +33,8 @@ void free_all(rf_handle *h) {
     void *ptrs[] = {h->tab, h->A64, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
                     h->PV32, h->PW32, h->vpart, h->pvx, h->pwx, h->work64, h->work32, h->r64, h->r32,
                     h->d32, h->x32, h->Pblocks, h->knn, h->mlp_w, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out,
-                    h->dscal, h->rb.partials, h->rb.counter};
+                    h->dscal, h->rb.partials, h->rb.counter, h->near_bits, h->near_list, h->near_cnt,
+                    h->far_contr, h->near_contr, h->near_pref, h->near_off, h->near_total, h->nearbuf};
     for (void *p : ptrs) cudaFree(p);
     h->gm64.reset();
     h->gm32.reset();
@@ -64,11 +65,14 @@ void make_tables(const rf_params &p, rf::Tables &t) {
         a = a + iv;
     }
     // Legendre polynomials at the points with the explicit formulas of
-    // compute_LVecs (matrix_assembly.f90:36-56); P_0 = 1
+    // compute_LVecs (matrix_assembly.f90:36-56); P_0 = 1.  Rows N+1, N+2 (when
+    // they fit) serve the split mixed-precision assembly, which projects onto
+    // P_0..P_{N+2}.
+    const int mmax = std::min(rf::kMaxN, N + 2);
     for (int q = 0; q < t.LQ; ++q) {
         const double x = t.pv[q];
         t.P[0][q] = 1.0;
-        for (int m = 1; m <= N; ++m) {
+        for (int m = 1; m <= mmax; ++m) {
             double v;
             switch (m) {
                 case 1: v = x; break;
@@ -289,6 +293,27 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
     CKC(cudaMemset(h->x, 0, h->n * 8), "memset x");
     CKC(cudaMemset(h->b, 0, h->n * 8), "memset b");
     CKC(dalloc(&h->bpart, (size_t)h->asm_chunks * h->n), "alloc rhs partials");
+    // the split assembly (FP32 far pairs, FP64 near pairs) for the reduced
+    // precisions with analytic integration; near_field_c >= 1e30 asks for FP64
+    // integrals everywhere and keeps the tile kernel
+    h->split = prec != RF_PREC_FP64 && p->use_analytical_integration != 0 && rf::split_supported(N, h->LQ) &&
+               !(prec != RF_PREC_FP32 && p->near_field_c >= 1e30);
+    if (h->split) {
+        h->far_chunks = rf::split_far_chunks(M, h->sm_count);
+        h->far_chunk = (M + h->far_chunks - 1) / h->far_chunks;
+        h->far_chunks = (M + h->far_chunk - 1) / h->far_chunk;
+        CKC(dalloc(&h->far_contr, (size_t)h->far_chunks * M * 3 * (N + 1)), "alloc rhs partials");
+        if (prec != RF_PREC_FP32) {
+            const size_t words = (M + 31) / 32;
+            CKC(dalloc(&h->near_bits, (size_t)M * words), "alloc near-pair bitmap");
+            CKC(dalloc(&h->near_list, (size_t)M * M), "alloc near-pair lists");
+            CKC(dalloc(&h->near_cnt, (size_t)M), "alloc near-pair counts");
+            CKC(dalloc(&h->near_pref, (size_t)M * words), "alloc near-pair prefix counts");
+            CKC(dalloc(&h->near_off, (size_t)M), "alloc near-pair offsets");
+            CKC(dalloc(&h->near_total, 1), "alloc near-pair counter");
+            CKC(dalloc(&h->near_contr, (size_t)M * 3 * (N + 1)), "alloc rhs partials");
+        }
+    }
     CKC(dalloc(&h->velpart, (size_t)h->vel_chunks * 6 * M), "alloc velocity partials");
     if (p->velocity_mode == RF_VEL_REUSE) {
         const size_t psz = (size_t)h->ldp * (size_t)h->n;
@@ -404,13 +429,73 @@ rf_status rf_assemble_system(rf_handle *h) {
         a.near_c = h->p.near_field_c > 0.0 ? h->p.near_field_c : 10.0;
         a.axis_ratio = 1.0 / 16.0;
     }
-    // near_field_c >= 1e30 keeps every integral in FP64 for the mixed paths
-    const int pmode = (prec == RF_PREC_FP64 || (prec != RF_PREC_FP32 && a.near_c >= 1e30)) ? rf::kPModeFP64
-                                                                                          : rf::kPModeMixed;
-    CK(h, rf::launch_assemble(a, h->p.use_analytical_integration == 0, pmode, h->asm_chunks, h->stream),
-       "assemble kernel");
-    CK(h, rf::launch_reduce_chunks(h->bpart, h->asm_chunks, h->n, h->n, h->b, h->stream), "rhs reduction");
-    h->launches += 2;
+    if (h->split) {
+        rf::SplitArgs sa{};
+        sa.M = h->M;
+        sa.N = h->N;
+        sa.LQ = h->LQ;
+        sa.pos = a.pos;
+        sa.ori = a.ori;
+        sa.tab = h->tab;
+        sa.A32 = h->A32;
+        sa.A16 = h->A16;
+        sa.lda = h->lda;
+        sa.PV32 = h->PV32;
+        sa.PW32 = h->PW32;
+        sa.ldp = h->ldp;
+        sa.near_bits = h->near_bits;
+        sa.words = (h->M + 31) / 32;
+        sa.near_list = h->near_list;
+        sa.near_cnt = h->near_cnt;
+        sa.near_pref = h->near_pref;
+        sa.near_off = h->near_off;
+        sa.near_total = h->near_total;
+        sa.far_contr = h->far_contr;
+        sa.near_contr = h->near_contr;
+        sa.chunk = h->far_chunk;
+        sa.near_c = a.near_c;
+        sa.axis_ratio = a.axis_ratio;
+        bool direct = false;
+        if (h->near_bits) {
+            CK(h, rf::launch_split_classify(sa, h->stream), "near-pair classification");
+            // the near-pair count sizes the buffer of FP64-integrated blocks
+            int *hcount = reinterpret_cast<int *>(h->hscal + 7);
+            CK(h, cudaMemcpyAsync(hcount, h->near_total, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+               "near-pair count");
+            CK(h, cudaStreamSynchronize(h->stream), "near-pair count");
+            h->near_pairs = *hcount;
+            if (h->near_pairs > h->near_cap) {
+                cudaFree(h->nearbuf);
+                h->nearbuf = nullptr;
+                h->near_cap = 0;
+                const int64_t cap = std::min<int64_t>((int64_t)h->M * (h->M - 1), h->near_pairs + h->near_pairs / 4 + 1024);
+                if (cudaMalloc(&h->nearbuf, sizeof(float) * rf::kNearBlockFloats * (size_t)cap) == cudaSuccess) {
+                    h->near_cap = cap;
+                } else {
+                    (void)cudaGetLastError();  // out of memory: write the near blocks into A directly
+                    h->nearbuf = nullptr;
+                }
+            }
+            direct = h->near_pairs > h->near_cap;
+            sa.nearbuf = h->nearbuf;
+            sa.merge = direct ? 0 : 1;
+            if (!direct) CK(h, rf::launch_split_near(sa, false, h->stream), "near-pair kernel");
+        }
+        CK(h, rf::launch_split_far(sa, h->far_chunks, h->stream), "far-pair kernel");
+        if (h->near_bits && direct) CK(h, rf::launch_split_near(sa, true, h->stream), "near-pair kernel");
+        CK(h, rf::launch_split_finish(sa, h->far_chunks, h->b, h->vpart, h->stream), "rhs finish");
+        h->vpart_chunks = 1;
+        h->launches += h->near_bits ? 4 : 2;
+    } else {
+        // near_field_c >= 1e30 keeps every integral in FP64 for the mixed paths
+        const int pmode = (prec == RF_PREC_FP64 || (prec != RF_PREC_FP32 && a.near_c >= 1e30)) ? rf::kPModeFP64
+                                                                                              : rf::kPModeMixed;
+        CK(h, rf::launch_assemble(a, h->p.use_analytical_integration == 0, pmode, h->asm_chunks, h->stream),
+           "assemble kernel");
+        CK(h, rf::launch_reduce_chunks(h->bpart, h->asm_chunks, h->n, h->n, h->b, h->stream), "rhs reduction");
+        h->vpart_chunks = h->asm_chunks;
+        h->launches += 2;
+    }
     if (h->p.preconditioner != RF_PC_NONE) {
         rf_status s = rf::build_preconditioner(h);
         if (s != RF_OK) return s;
@@ -574,7 +659,7 @@ rf_status rf_update_velocities(rf_handle *h) {
                                                                    h->work64, h->work_elems, h->sm_count, st)),
                "velocity panel");
         }
-        CK(h, rf::launch_velocity_reuse_finish(h->M, h->T[h->cur], h->tab, h->pvx, h->pwx, h->vpart, h->asm_chunks,
+        CK(h, rf::launch_velocity_reuse_finish(h->M, h->T[h->cur], h->tab, h->pvx, h->pwx, h->vpart, h->vpart_chunks,
                                                V, W, st),
            "velocity finish");
         h->launches += 5;

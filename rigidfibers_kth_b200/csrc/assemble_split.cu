@@ -1,0 +1,945 @@
+// assemble_split.cu - mixed-precision assembly split by pair distance.
+//
+// Reference: fortran/matrix_assembly.f90:407-629 (matrix, analytic) and
+// 796-905 (right-hand side); Int_analytical.f90:72-288 (inner integral).
+//
+// The mixed path stores A in FP32 (and BF16).  A fiber pair (i, j) is "near"
+// when one of target i's quadrature points lies within sqrt(near_c) of source
+// j's centre or close to its axis beyond its ends (the forward-recursion range
+// of the reference, c < 10, and the cancellation-prone closed forms).  Near
+// pairs (about a sixth of the pairs in a dense cloud) are integrated in FP64,
+// far pairs in FP32.  Three kernels:
+//   classify_kernel   one warp per target: near-pair bitmap and per-target
+//                     lists in ascending source order;
+//   far_pairs_kernel  FP32, lane = target fiber, warp-uniform source: every
+//                     lane integrates its own pair over the target's Gauss
+//                     points with the projection accumulated in registers,
+//                     then stages the 3N x 3N block in shared memory and the
+//                     warp writes whole column segments;
+//   near_pairs_kernel FP64, one warp per near pair: lane = Gauss point, the
+//                     projection on the FP64 tensor cores (mma.sync m8n8k4).
+// A finish kernel sums the per-chunk right-hand-side partials in a fixed order.
+//
+// Projection without forming the tensors.  The reference forms, per target
+// point q and source weight m, G_m(q) = cI I + cRR R0R0 + cPR (pR0 + R0p)
+// + cPP pp and projects theta^k_m = sum_q w_q P_k(s_q) G_m(q).  Here
+//   cI  = sc_m sum_p a_mp u_p,        u_p = I_p + 2 eps^2 J_p
+//   cRR = sc_m sum_p a_mp v_p,        v_p = J_p - 6 eps^2 S_p
+//   cPR = -sc_m sum_p a_mp v_{p+1},   cPP = sc_m sum_p a_mp v_{p+2}
+// (a_mp, sc_m the Legendre coefficients of Int_analytical.f90:213-288), and
+// R0 = D + s_q t with D = x_i - x_j, t = t_i, so every entry of theta is a
+// combination of the scalar projections <u_p>_k, <v_p>_k, <s v_p>_k and
+// <s^2 v_p>_k times the seven pair tensors I, DD, Dt+tD, tt, pD+Dp, pt+tp,
+// pp.  Bonnet's recursion s P_k = ((k+1) P_{k+1} + k P_{k-1}) / (2k+1) holds
+// at every point, so <s f>_k = alpha_k <f>_{k+1} + beta_k <f>_{k-1}: the
+// per-point work is 2N+4 scalars projected onto P_0..P_{N+2}, the same sums in
+// another order.
+#include <algorithm>
+
+#include "rf_kernels.h"
+
+namespace rf {
+
+namespace {
+
+template <int N>
+struct SplitDims {
+    static constexpr int NL = N + 1;          // u_p and Legendre indices 0..N
+    static constexpr int NV = N + 3;          // v_p, p = 0..N+2
+    static constexpr int KW = N + 3;          // projection rows k = 0..N+2
+    static constexpr int NC = NL + NV;        // scalars per Gauss point
+    static constexpr int RB = 3 * N;          // rows (and columns) of a pair block
+    static constexpr int NRHS = 3 * NL;       // theta^k_0 f, k = 0..N
+};
+
+// number of projection rows kept for v_p
+__host__ __device__ constexpr int vrows(int N, int p) { return p <= N ? N + 3 : (p == N + 1 ? N + 2 : N + 1); }
+
+__host__ __device__ constexpr double bonnet_a(int k) { return (k + 1.0) / (2.0 * k + 1.0); }
+__host__ __device__ constexpr double bonnet_b(int k) { return k / (2.0 * k + 1.0); }
+
+// Scalar coefficient sets of source weight m from the projections
+// U(p, k) = <u_p>_k and V(p, k) = <v_p>_k.
+template <typename T, int N>
+struct LegSets {
+    T AI[N + 1], R0[N + 3], R1[N + 2], R2[N + 1], C0[N + 2], C1[N + 1], E[N + 1];
+};
+
+template <typename T, int N, int m, typename UF, typename VF>
+__device__ __forceinline__ void leg_sets(const UF &U, const VF &V, LegSets<T, N> &o) {
+    const T sc = (T)leg_scale(m);
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+        T s = 0;
+#pragma unroll
+        for (int p = m; p >= 0; --p)
+            if (leg_coef(m, p) != 0) s += (T)leg_coef(m, p) * U(p, k);
+        o.AI[k] = sc * s;
+    }
+#pragma unroll
+    for (int k = 0; k <= N + 2; ++k) {
+        T s = 0;
+#pragma unroll
+        for (int p = m; p >= 0; --p)
+            if (leg_coef(m, p) != 0) s += (T)leg_coef(m, p) * V(p, k);
+        o.R0[k] = sc * s;
+    }
+#pragma unroll
+    for (int k = 0; k <= N + 1; ++k) {
+        T s = 0;
+#pragma unroll
+        for (int p = m; p >= 0; --p)
+            if (leg_coef(m, p) != 0) s += (T)leg_coef(m, p) * V(p + 1, k);
+        o.C0[k] = -sc * s;
+    }
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+        T s = 0;
+#pragma unroll
+        for (int p = m; p >= 0; --p)
+            if (leg_coef(m, p) != 0) s += (T)leg_coef(m, p) * V(p + 2, k);
+        o.E[k] = sc * s;
+    }
+#pragma unroll
+    for (int k = 0; k <= N + 1; ++k)
+        o.R1[k] = (T)bonnet_a(k) * o.R0[k + 1] + (k > 0 ? (T)bonnet_b(k) * o.R0[k > 0 ? k - 1 : 0] : (T)0);
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+        o.R2[k] = (T)bonnet_a(k) * o.R1[k + 1] + (k > 0 ? (T)bonnet_b(k) * o.R1[k > 0 ? k - 1 : 0] : (T)0);
+        o.C1[k] = (T)bonnet_a(k) * o.C0[k + 1] + (k > 0 ? (T)bonnet_b(k) * o.C0[k > 0 ? k - 1 : 0] : (T)0);
+    }
+}
+
+// The seven pair tensors, packed 11,22,33,12,13,23 (identity implicit).
+template <typename T>
+struct PairTensors {
+    T DD[6], DT[6], TT[6], PD[6], PT[6], PP[6];
+    __device__ __forceinline__ void set(const T *D, const T *t, const T *p) {
+        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const int x = ia[c], y = ib[c];
+            DD[c] = D[x] * D[y];
+            DT[c] = D[x] * t[y] + t[x] * D[y];
+            TT[c] = t[x] * t[y];
+            PD[c] = p[x] * D[y] + D[x] * p[y];
+            PT[c] = p[x] * t[y] + t[x] * p[y];
+            PP[c] = p[x] * p[y];
+        }
+    }
+    // theta for projection row k of the sets
+    template <int N>
+    __device__ __forceinline__ void theta(const LegSets<T, N> &s, int k, T *th) const {
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            th[c] = (c < 3 ? s.AI[k] : (T)0) + s.R0[k] * DD[c] + s.R1[k] * DT[c] + s.R2[k] * TT[c] +
+                    s.C0[k] * PD[c] + s.C1[k] * PT[c] + s.E[k] * PP[c];
+    }
+};
+
+// FP64 moments for the near pairs of the mixed path: the reference formulas
+// (Int_analytical.f90:96-207) with ordinary (contracted) arithmetic and the
+// loop-constant divisions folded into reciprocals.
+template <int N>
+__device__ __forceinline__ void moments_near(double b, double c, double *I, double *J, double *S) {
+    constexpr int K = N + 3;
+    const double ue = sqrt(1.0 + b + c);
+    const double ub = sqrt(1.0 - b + c);
+    const double te = 1.0 + 0.5 * b;
+    const double tb = -1.0 + 0.5 * b;
+    const double d = c - 0.25 * b * b;
+    const double iue = 1.0 / ue, iub = 1.0 / ub;
+    I[0] = log(fabs(2.0 + b + 2.0 * ue)) - log(fabs(-2.0 + b + 2.0 * ub));
+    I[1] = ue - ub - 0.5 * b * I[0];
+    if (d < 1e-14) {
+        const double e1 = 1.0 + 0.5 * b, e2 = -1.0 + 0.5 * b;
+        J[0] = -0.5 / (e1 * e1) + 0.5 / (e2 * e2);
+        J[1] = -iue + iub - 0.5 * b * J[0];
+        const double p = 2.0 + b, m = -2.0 + b;
+        const double p2 = p * p, m2 = m * m;
+        S[0] = -4.0 / (p2 * p2) + 4.0 / (m2 * m2);
+        S[1] = -8.0 / (3.0 * p2 * p) + 8.0 / (3.0 * m2 * m) - 0.5 * b * S[0];
+    } else {
+        const double id = 1.0 / d;
+        J[0] = (te * iue - tb * iub) * id;
+        J[1] = -iue + iub - 0.5 * b * J[0];
+        const double iue3 = iue * iue * iue, iub3 = iub * iub * iub;
+        const double id6 = id * (1.0 / 6.0);
+        S[0] = ((2.0 + b) * iue3 - (-2.0 + b) * iub3) * id6 + (2.0 / 3.0) * id * J[0];
+        S[1] = (-(b + 2.0 * c) * iue3 + (-b + 2.0 * c) * iub3) * id6 - (1.0 / 3.0) * b * id * J[0];
+    }
+    if (c < 10.0) {
+#pragma unroll
+        for (int n = 2; n < K; ++n) {
+            const double nn = n + 1.0;
+            const double r = 1.0 / (1.0 - nn);
+            const double sbp = (n % 2 == 1) ? 1.0 : -1.0;
+            I[n] = (sbp * r) * ub - r * ue - ((0.5 - (nn - 1.0)) * r) * b * I[n - 1] + ((nn - 2.0) * r) * c * I[n - 2];
+            J[n] = I[n - 2] - b * J[n - 1] - c * J[n - 2];
+            S[n] = J[n - 2] - b * S[n - 1] - c * S[n - 2];
+        }
+    } else {
+        const double ic = 1.0 / c;
+        double i1 = 0.0, i2 = 0.0, j1 = 0.0, j2 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll
+        for (int n = 27; n >= 2; --n) {
+            const double nn = n;
+            const double a0 = (nn + 2.0) / (nn + 1.0);
+            const double r2 = 1.0 / (nn + 2.0);
+            const double cb = (1.0 - 2.0 * (nn + 2.0)) / (2.0 * (nn + 2.0));
+            const double sbp = ((n + 1) % 2 == 0) ? 1.0 : -1.0;
+            const double in = a0 * ic * (ue * r2 - sbp * ub * r2 + cb * b * i1 - i2);
+            const double jn = ic * (in - b * j1 - j2);
+            const double sn = ic * (jn - b * s1 - s2);
+            if (n < K) { I[n] = in; J[n] = jn; S[n] = sn; }
+            i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
+        }
+    }
+}
+
+// Near-pair buffer: per pair and source weight m = 1..N a 64-float record
+// (16-byte aligned): the block columns 3(m-1)..3(m-1)+2 [col][row] (9N
+// floats), then the velocity panel entries [w][col][a] (18 floats).
+constexpr int kNearWeight = 64;
+constexpr int kNearBlock = 5 * kNearWeight;
+static_assert(9 * 5 + 18 <= kNearWeight, "near record");
+
+// ---------------------------------------------------------------- classify
+constexpr int kClassifyWarps = 4;
+
+// One warp per target: the near-pair bitmap, the number of near sources before
+// each bitmap word, the near sources in ascending order and their count, and
+// the target's first slot in the near-pair buffer (claimed with an atomic add;
+// slots only place the blocks, they do not change any value).
+__global__ void __launch_bounds__(kClassifyWarps * 32) classify_kernel(SplitArgs a) {
+    __shared__ double s_pv[kMaxLQ];
+    for (int t = threadIdx.x; t < kMaxLQ; t += blockDim.x) s_pv[t] = t < a.LQ ? a.tab->pv[t] : 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = blockIdx.x * kClassifyWarps + warp;
+    if (i >= a.M) return;  // whole warp
+    const double xi0 = a.pos[3 * i], xi1 = a.pos[3 * i + 1], xi2 = a.pos[3 * i + 2];
+    const double ti0 = a.ori[3 * i], ti1 = a.ori[3 * i + 1], ti2 = a.ori[3 * i + 2];
+    int count = 0;
+    int *list = a.near_list + (int64_t)i * a.M;
+    for (int jw = 0; jw < a.words; ++jw) {
+        const int j = jw * 32 + lane;
+        bool near = false;
+        if (j < a.M && j != i) {
+            const double D0 = xi0 - a.pos[3 * j], D1 = xi1 - a.pos[3 * j + 1], D2 = xi2 - a.pos[3 * j + 2];
+            const double p0 = a.ori[3 * j], p1 = a.ori[3 * j + 1], p2 = a.ori[3 * j + 2];
+            for (int q = 0; q < a.LQ && !near; ++q) {
+                const double s = s_pv[q];
+                const double r0 = D0 + s * ti0, r1 = D1 + s * ti1, r2 = D2 + s * ti2;
+                const double c = r0 * r0 + r1 * r1 + r2 * r2;
+                const double b = -2.0 * (p0 * r0 + p1 * r1 + p2 * r2);
+                const double d = c - 0.25 * b * b;
+                near = (c < a.near_c) || (d < c * a.axis_ratio);
+            }
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, near);
+        if (lane == 0) {
+            a.near_bits[(int64_t)i * a.words + jw] = mask;
+            a.near_pref[(int64_t)i * a.words + jw] = count;
+        }
+        if (near) list[count + __popc(mask & ((1u << lane) - 1u))] = j;
+        count += __popc(mask);
+    }
+    if (lane == 0) {
+        a.near_cnt[i] = count;
+        a.near_off[i] = atomicAdd(a.near_total, count);
+    }
+}
+
+// ---------------------------------------------------------------- far pairs (FP32)
+// One warp per CTA; lane = target fiber, the warp walks a chunk of sources.
+// For source weight m the block entries follow from
+//   theta = AI I + D X^T + t Y^T + p Z^T,   X = R0 D + R1 t + C0 p,
+//   Y = R1 D + R2 t + C1 p,  Z = C0 D + C1 t + E p,
+//   Q = theta t = AI t + (D.t) X + (t.t) Y + (p.t) Z,
+// the pair tensors of the header expanded.  The m loop runs at run time with
+// the Legendre coefficients sc_m a_mp in constant memory, which keeps the
+// kernel small enough for the instruction cache.
+
+#define RF_LEG(m, p) ((float)(leg_scale(m) * leg_coef(m, p)))
+#define RF_LEG_ROW(m) RF_LEG(m, 0), RF_LEG(m, 1), RF_LEG(m, 2), RF_LEG(m, 3), RF_LEG(m, 4), RF_LEG(m, 5), RF_LEG(m, 6), RF_LEG(m, 7)
+__constant__ float c_leg32[8][8] = {{RF_LEG_ROW(0)}, {RF_LEG_ROW(1)}, {RF_LEG_ROW(2)}, {RF_LEG_ROW(3)},
+                                    {RF_LEG_ROW(4)}, {RF_LEG_ROW(5)}, {RF_LEG_ROW(6)}, {RF_LEG_ROW(7)}};
+#undef RF_LEG_ROW
+#undef RF_LEG
+
+#ifndef RF_FAR_MINB
+#define RF_FAR_MINB 8
+#endif
+
+template <int N, bool PANELS>
+struct FarSmem {
+    static constexpr int GR = 32 * 3 * N;                   // staged rows of one column
+    static constexpr int PAN = 2 * 3 * 96;                  // staged panel columns
+    static constexpr int SET = (N + 1) * 7 * 32;            // coefficient sets of one weight [k][7][lane]
+    static size_t bytes() {
+        return sizeof(float) * (32 * kNearWeight + SET + 16 + 64 + kMaxLQ + kMaxLQ * SplitDims<N>::KW + 3 * GR +
+                                (PANELS ? PAN : 0));
+    }
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int N, bool PANELS>
+__device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, int i0, int nvalid, const float *stg,
+                                            const float *pan, int lane) {
+    constexpr int RB = 3 * N, GR = 32 * RB;
+    const int64_t row0 = (int64_t)i0 * RB;
+    const int nrows = nvalid * RB;
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+        const int64_t col = (int64_t)j * RB + 3 * (m - 1) + bb;
+        const float *src = stg + bb * GR;
+        if (nrows == GR) {
+            const float4 *s4 = reinterpret_cast<const float4 *>(src);
+            if (a.A32) {
+                float4 *d4 = reinterpret_cast<float4 *>(a.A32 + col * a.lda + row0);
+                for (int e = lane; e < GR / 4; e += 32) d4[e] = s4[e];
+            }
+            if (a.A16) {
+                uint2 *d2 = reinterpret_cast<uint2 *>(a.A16 + col * a.lda + row0);
+                for (int e = lane; e < GR / 4; e += 32) {
+                    const float4 v = s4[e];
+                    __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+                    uint2 u;
+                    u.x = *reinterpret_cast<unsigned *>(&lo);
+                    u.y = *reinterpret_cast<unsigned *>(&hi);
+                    d2[e] = u;
+                }
+            }
+        } else {
+            for (int e = lane; e < nrows; e += 32) {
+                if (a.A32) a.A32[col * a.lda + row0 + e] = src[e];
+                if (a.A16) a.A16[col * a.lda + row0 + e] = __float2bfloat16_rn(src[e]);
+            }
+        }
+        if (PANELS) {
+            const int prow = 3 * nvalid;
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                float *dst = (w ? a.PW32 : a.PV32) + col * a.ldp + (int64_t)i0 * 3;
+                const float *ps = pan + (w * 3 + bb) * 96;
+                if (prow == 96) {
+                    if (lane < 24) reinterpret_cast<float4 *>(dst)[lane] = reinterpret_cast<const float4 *>(ps)[lane];
+                } else {
+                    for (int e = lane; e < prow; e += 32) dst[e] = ps[e];
+                }
+            }
+        }
+    }
+}
+
+template <int N, bool PANELS, bool FAR>
+__global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a) {
+    using SD = SplitDims<N>;
+    using SM = FarSmem<N, PANELS>;
+    constexpr int NL = SD::NL, NV = SD::NV, KW = SD::KW, NRHS = SD::NRHS, RB = SD::RB, GR = SM::GR;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x;
+    float *s_nb = reinterpret_cast<float *>(smem_raw);               // [near lane][kNearWeight], one weight
+    float *s_set = s_nb + 32 * kNearWeight;                           // [k][7][32]
+    float *s_gk = s_set + SM::SET;                                    // gamma_k (0..7), E_k (8..15)
+    int *s_nl = reinterpret_cast<int *>(s_gk + 16);                   // near lanes of the source, in order
+    int *s_ns = s_nl + 32;                                            // and their buffer slots
+    float *s_pv = reinterpret_cast<float *>(s_ns + 32);
+    float *s_w = s_pv + kMaxLQ;                                       // [kMaxLQ][KW]: w_q P_k(s_q)
+    float *s_stg = s_w + kMaxLQ * KW;                                 // [3][GR]
+    float *s_pan = s_stg + 3 * GR;                                    // [2][3][96]
+
+    const Tables &tab = *a.tab;
+    const int LQ = a.LQ;
+    for (int t = lane; t < kMaxLQ; t += 32) s_pv[t] = t < LQ ? (float)tab.pv[t] : 0.f;
+    for (int t = lane; t < kMaxLQ * KW; t += 32) {
+        const int q = t / KW, k = t - q * KW;
+        s_w[t] = q < LQ ? (float)(tab.wv[q] * tab.P[k][q]) : 0.f;
+    }
+    if (lane < 8) {
+        s_gk[lane] = lane <= N ? (float)tab.gamma[lane] : 0.f;
+        s_gk[8 + lane] = lane <= N ? (float)tab.Ek[lane] : 0.f;
+    }
+    double rhs[NRHS];  // sum over the far sources of theta^k_0 f
+#pragma unroll
+    for (int r = 0; r < NRHS; ++r) rhs[r] = 0.0;
+    __syncwarp();
+
+    const float D1 = (float)tab.D1, sv = (float)(0.5 / tab.d), sw = (float)(1.5 / tab.d);
+    const float f[3] = {(float)tab.half_force[0], (float)tab.half_force[1], (float)tab.half_force[2]};
+    const float e2 = (float)(2.0 * tab.eps2), e6 = (float)(6.0 * tab.eps2);
+
+    const int i0 = blockIdx.x * 32;
+    const int i = i0 + lane;
+    const bool valid = i < a.M;
+    const int nvalid = min(32, a.M - i0);
+    const int ic = valid ? i : i0;
+    const double xi0 = a.pos[3 * ic], xi1 = a.pos[3 * ic + 1], xi2 = a.pos[3 * ic + 2];
+    const float t[3] = {(float)a.ori[3 * ic], (float)a.ori[3 * ic + 1], (float)a.ori[3 * ic + 2]};
+    const float tt = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+    const int64_t brow = (int64_t)ic * a.words;
+    const int slot0 = (valid && a.near_bits) ? a.near_off[ic] : 0;
+    const bool merge = a.near_bits != nullptr && a.merge != 0;
+
+    const int j0 = blockIdx.y * a.chunk;
+    const int j1 = min(a.M, j0 + a.chunk);
+    // the source's centre and direction are loaded one source ahead
+    double xj[3] = {0.0, 0.0, 0.0};
+    float pj[3] = {0.f, 0.f, 0.f};
+    if (j0 < j1) {
+        xj[0] = __ldg(a.pos + 3 * j0); xj[1] = __ldg(a.pos + 3 * j0 + 1); xj[2] = __ldg(a.pos + 3 * j0 + 2);
+        pj[0] = (float)__ldg(a.ori + 3 * j0); pj[1] = (float)__ldg(a.ori + 3 * j0 + 1); pj[2] = (float)__ldg(a.ori + 3 * j0 + 2);
+    }
+    unsigned word = 0u;
+    int wpref = 0;
+    for (int j = j0; j < j1; ++j) {
+        const float D[3] = {(float)(xi0 - xj[0]), (float)(xi1 - xj[1]), (float)(xi2 - xj[2])};
+        const float p[3] = {pj[0], pj[1], pj[2]};
+        if (j + 1 < j1) {
+            xj[0] = __ldg(a.pos + 3 * j + 3); xj[1] = __ldg(a.pos + 3 * j + 4); xj[2] = __ldg(a.pos + 3 * j + 5);
+            pj[0] = (float)__ldg(a.ori + 3 * j + 3); pj[1] = (float)__ldg(a.ori + 3 * j + 4); pj[2] = (float)__ldg(a.ori + 3 * j + 5);
+        }
+        bool near = false;
+        int slot = 0;
+        if (valid && a.near_bits) {
+            if (j == j0 || (j & 31) == 0) {
+                word = a.near_bits[brow + (j >> 5)];
+                wpref = merge ? a.near_pref[brow + (j >> 5)] : 0;
+            }
+            near = (word >> (j & 31)) & 1u;
+            if (near) slot = slot0 + wpref + __popc(word & ((1u << (j & 31)) - 1u));
+        }
+        const unsigned nmask = merge ? __ballot_sync(0xffffffffu, near) : 0u;
+        const int nnear = __popc(nmask);
+        // list the near lanes in order and prefetch their weight-1 records;
+        // the Gauss-point loop hides the copy
+        if (near && merge) {
+            const int r = __popc(nmask & ((1u << lane) - 1u));
+            s_nl[r] = lane;
+            s_ns[r] = slot;
+        }
+        __syncwarp();
+        for (int u = lane; u < nnear * (kNearWeight / 4); u += 32) {
+            const int r = u / (kNearWeight / 4), c = u - r * (kNearWeight / 4);
+            cp_async16(s_nb + r * kNearWeight + 4 * c, a.nearbuf + (int64_t)s_ns[r] * kNearBlock + 4 * c);
+        }
+        cp_async_commit();
+        const bool diag = i == j;
+        const bool act = valid && !near && !diag;
+
+        float U[NL][NL], V[NV][KW];
+#pragma unroll
+        for (int pp = 0; pp < NL; ++pp)
+#pragma unroll
+            for (int k = 0; k < NL; ++k) U[pp][k] = 0.f;
+#pragma unroll
+        for (int pp = 0; pp < NV; ++pp)
+#pragma unroll
+            for (int k = 0; k < KW; ++k) V[pp][k] = 0.f;
+        if (act) {
+            for (int q = 0; q < LQ; ++q) {
+                const float sq = s_pv[q];
+                const float r0x = fmaf(sq, t[0], D[0]), r0y = fmaf(sq, t[1], D[1]), r0z = fmaf(sq, t[2], D[2]);
+                const float b = -2.0f * (p[0] * r0x + p[1] * r0y + p[2] * r0z);
+                const float c = r0x * r0x + r0y * r0y + r0z * r0z;
+                float I[KW], J[KW], S[KW];
+                moments_fp32<N, FAR>(b, c, I, J, S);
+                const float *w = s_w + q * KW;
+                float wk[KW];
+#pragma unroll
+                for (int k = 0; k < KW; ++k) wk[k] = w[k];
+#pragma unroll
+                for (int pp = 0; pp < NL; ++pp) {
+                    const float u = fmaf(e2, J[pp], I[pp]);
+#pragma unroll
+                    for (int k = 0; k < NL; ++k) U[pp][k] = fmaf(wk[k], u, U[pp][k]);
+                }
+#pragma unroll
+                for (int pp = 0; pp < NV; ++pp) {
+                    const float v = fmaf(-e6, S[pp], J[pp]);
+#pragma unroll
+                    for (int k = 0; k < KW; ++k)
+                        if (k < vrows(N, pp)) V[pp][k] = fmaf(wk[k], v, V[pp][k]);
+                }
+            }
+        }
+        const float Dt = D[0] * t[0] + D[1] * t[1] + D[2] * t[2];
+        const float pt = p[0] * t[0] + p[1] * t[1] + p[2] * t[2];
+        cp_async_wait_all();
+        __syncwarp();
+
+        if (act) {
+            // right-hand side: theta^k_0 f for weight 0 (near pairs add theirs in the near kernel)
+#pragma unroll
+            for (int k = 0; k <= N; ++k) {
+                float R0[3] = {0.f, 0.f, 0.f}, C0[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+                for (int o = 0; o < 3; ++o) {
+                    const int kk = k - 1 + o;
+                    if (kk >= 0) C0[o] = -V[1][kk];
+                }
+                const float AI = U[0][k], E = V[2][k];
+                const float R0k = V[0][k], R0p = V[0][k + 1], R0pp = V[0][k + 2];
+                const float R0m = k > 0 ? V[0][k > 0 ? k - 1 : 0] : 0.f, R0mm = k > 1 ? V[0][k > 1 ? k - 2 : 0] : 0.f;
+                const float R1 = (float)bonnet_a(k) * R0p + (float)bonnet_b(k) * R0m;
+                const float R1p = (float)bonnet_a(k + 1) * R0pp + (float)bonnet_b(k + 1) * R0k;
+                const float R1m = k > 0 ? (float)bonnet_a(k - 1) * R0k + (float)bonnet_b(k - 1) * R0mm : 0.f;
+                const float R2 = (float)bonnet_a(k) * R1p + (float)bonnet_b(k) * R1m;
+                const float C1 = (float)bonnet_a(k) * C0[2] + (float)bonnet_b(k) * C0[0];
+                (void)R0;
+                float X[3], Y[3], Z[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    X[c] = R0k * D[c] + R1 * t[c] + C0[1] * p[c];
+                    Y[c] = R1 * D[c] + R2 * t[c] + C1 * p[c];
+                    Z[c] = C0[1] * D[c] + C1 * t[c] + E * p[c];
+                }
+                const float Xf = X[0] * f[0] + X[1] * f[1] + X[2] * f[2];
+                const float Yf = Y[0] * f[0] + Y[1] * f[1] + Y[2] * f[2];
+                const float Zf = Z[0] * f[0] + Z[1] * f[1] + Z[2] * f[2];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) rhs[3 * k + c] += (double)(AI * f[c] + D[c] * Xf + t[c] * Yf + p[c] * Zf);
+            }
+        }
+
+#pragma unroll 1
+        for (int m = 1; m <= N; ++m) {
+            // coefficient sets of weight m for rows k = 0..N, staged per lane
+            {
+                float cf[NL];
+#pragma unroll
+                for (int pp = 0; pp < NL; ++pp) cf[pp] = c_leg32[m][pp];
+                float R0[N + 3], C0[N + 2], R1[N + 2];
+#pragma unroll
+                for (int k = 0; k < N + 3; ++k) {
+                    float s1 = 0.f;
+#pragma unroll
+                    for (int pp = 0; pp < NL; ++pp) s1 = fmaf(cf[pp], V[pp][k], s1);
+                    R0[k] = s1;
+                }
+#pragma unroll
+                for (int k = 0; k < N + 2; ++k) {
+                    float s1 = 0.f;
+#pragma unroll
+                    for (int pp = 0; pp < NL; ++pp) s1 = fmaf(cf[pp], V[pp + 1][k], s1);
+                    C0[k] = -s1;
+                }
+#pragma unroll
+                for (int k = 0; k < N + 2; ++k)
+                    R1[k] = (float)bonnet_a(k) * R0[k + 1] + (k > 0 ? (float)bonnet_b(k) * R0[k > 0 ? k - 1 : 0] : 0.f);
+#pragma unroll
+                for (int k = 0; k < NL; ++k) {
+                    float ai = 0.f, ee = 0.f;
+#pragma unroll
+                    for (int pp = 0; pp < NL; ++pp) {
+                        ai = fmaf(cf[pp], U[pp][k], ai);
+                        ee = fmaf(cf[pp], V[pp + 2][k], ee);
+                    }
+                    float *o = s_set + k * 7 * 32 + lane;
+                    o[0] = ai;
+                    o[32] = R0[k];
+                    o[64] = R1[k];
+                    o[96] = (float)bonnet_a(k) * R1[k + 1] + (k > 0 ? (float)bonnet_b(k) * R1[k > 0 ? k - 1 : 0] : 0.f);
+                    o[128] = C0[k];
+                    o[160] = (float)bonnet_a(k) * C0[k + 1] + (k > 0 ? (float)bonnet_b(k) * C0[k > 0 ? k - 1 : 0] : 0.f);
+                    o[192] = ee;
+                }
+            }
+#pragma unroll 1
+            for (int k = 0; k <= N; ++k) {
+                const float *o = s_set + k * 7 * 32 + lane;
+                const float AI = o[0], R0 = o[32], R1 = o[64], R2 = o[96], C0 = o[128], C1 = o[160], E = o[192];
+                float X[3], Y[3], Z[3], Q[3];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    X[c] = R0 * D[c] + R1 * t[c] + C0 * p[c];
+                    Y[c] = R1 * D[c] + R2 * t[c] + C1 * p[c];
+                    Z[c] = C0 * D[c] + C1 * t[c] + E * p[c];
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c) Q[c] = AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c];
+                if (k >= 1) {
+                    const float g = s_gk[k], ek = s_gk[8 + k];
+                    float *dst = s_stg + lane * RB + 3 * (k - 1);
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                        for (int aa = 0; aa < 3; ++aa) {
+                            float v = (k == 1) ? D1 * t[aa] * Q[bb]
+                                               : g * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] +
+                                                      t[aa] * (Y[bb] - ek * Q[bb]) + p[aa] * Z[bb]);
+                            if (diag) v = (k == m && aa == bb) ? 1.f : 0.f;
+                            dst[bb * GR + aa] = v;
+                        }
+                }
+                if (PANELS && k <= 1) {
+#pragma unroll
+                    for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                        for (int aa = 0; aa < 3; ++aa) {
+                            const float th = (aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * Y[bb] + p[aa] * Z[bb];
+                            const float v = (k == 0) ? sv * th : sw * (th - Q[bb] * t[aa]);
+                            s_pan[(k * 3 + bb) * 96 + lane * 3 + aa] = diag ? 0.f : v;
+                        }
+                }
+            }
+            cp_async_wait_all();
+            __syncwarp();
+            // near pairs: the FP64-integrated columns of weight m replace the
+            // staged zeros, one (near lane, entry) per thread
+            {
+                constexpr int PER = 3 * RB + (PANELS ? 18 : 0);
+                for (int idx = lane; idx < nnear * PER; idx += 32) {
+                    const int r = idx / PER, e = idx - r * PER;
+                    const int L = s_nl[r];
+                    int dst;
+                    if (e < 3 * RB) {
+                        const int bb = e / RB, rr = e - bb * RB;
+                        dst = bb * GR + L * RB + rr;
+                    } else {
+                        const int e2 = e - 3 * RB, w = e2 / 9, rem = e2 - w * 9, bb = rem / 3, aa = rem - bb * 3;
+                        dst = 3 * GR + (w * 3 + bb) * 96 + L * 3 + aa;  // s_pan follows s_stg
+                    }
+                    s_stg[dst] = s_nb[r * kNearWeight + e];
+                }
+            }
+            __syncwarp();
+            // the records of weight m+1, hidden behind the stores and the next weight
+            if (m < N) {
+                for (int u = lane; u < nnear * (kNearWeight / 4); u += 32) {
+                    const int r = u / (kNearWeight / 4), c = u - r * (kNearWeight / 4);
+                    cp_async16(s_nb + r * kNearWeight + 4 * c,
+                               a.nearbuf + (int64_t)s_ns[r] * kNearBlock + m * kNearWeight + 4 * c);
+                }
+                cp_async_commit();
+            }
+            far_store_m<N, PANELS>(a, m, j, i0, nvalid, s_stg, s_pan, lane);
+            __syncwarp();
+        }
+    }
+    if (valid) {
+#pragma unroll
+        for (int r = 0; r < NRHS; ++r) a.far_contr[((int64_t)blockIdx.y * a.M + i) * NRHS + r] = rhs[r];
+    }
+}
+
+// ---------------------------------------------------------------- near pairs (FP64)
+constexpr int kNearWarps = 4;
+constexpr int kXq = 52;  // q stride of X[col][q]: 52 = 4 mod 16 makes the B fragments conflict-free
+
+template <int N>
+struct NearSmem {
+    static constexpr int X = 16 * kXq;                  // per-point scalars [col][q], cols >= 2N+4 zero
+    static constexpr int TM = 8 * 16;                   // projections [k][col]
+    static constexpr int BLK = kNearBlock / 2;          // staged block + panels (floats)
+    static constexpr int RHS = 3 * (N + 1) + 1;
+    static constexpr int WARP = X + TM + BLK + RHS + ((X + TM + BLK + RHS) & 1);
+    static constexpr int TABLES = 8 * kMaxLQ + kMaxLQ + 64 + 16;   // w P, s, Legendre coefficients, Bonnet
+    static size_t bytes() { return sizeof(double) * (TABLES + (size_t)kNearWarps * WARP); }
+};
+
+// One CTA per target fiber, warps over its near sources.  Per pair: lane =
+// Gauss point for the FP64 moments, the projection on the tensor cores, then
+// lane = (source weight m, target row k) for the block entries.  The block
+// goes to the near-pair buffer (DIRECT = false; the far kernel merges it into
+// its column stores) or straight into A (DIRECT = true, used when the buffer
+// could not be grown).
+template <int N, bool PANELS, bool DIRECT>
+__global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a) {
+    using SD = SplitDims<N>;
+    using SM = NearSmem<N>;
+    constexpr int NL = SD::NL, NV = SD::NV, RB = SD::RB, NRHS = SD::NRHS;
+    constexpr int KSMAX = kMaxLQ / 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double *s_wP = reinterpret_cast<double *>(smem_raw);   // [8][kMaxLQ]
+    double *s_pv = s_wP + 8 * kMaxLQ;
+    double *s_leg = s_pv + kMaxLQ;                          // [8][8]: sc_m a_mp
+    double *s_bon = s_leg + 64;                             // alpha_k (0..7), beta_k (8..15)
+    double *base = s_wP + SM::TABLES + (size_t)warp * SM::WARP;
+    double *X = base;
+    double *Tm = X + SM::X;
+    float *blk = reinterpret_cast<float *>(Tm + SM::TM);    // [col][row] RB*RB, then panels [w][col][a]
+    double *rhs = Tm + SM::TM + SM::BLK;
+
+    const Tables &tab = *a.tab;
+    const int LQ = a.LQ;
+    const int KS = (LQ + 3) / 4;
+    for (int t = threadIdx.x; t < 8 * kMaxLQ; t += blockDim.x) {
+        const int k = t / kMaxLQ, q = t - k * kMaxLQ;
+        s_wP[t] = (k < SD::KW && q < LQ) ? tab.wv[q] * tab.P[k][q] : 0.0;
+    }
+    for (int t = threadIdx.x; t < kMaxLQ; t += blockDim.x) s_pv[t] = t < LQ ? tab.pv[t] : 0.0;
+    for (int t = threadIdx.x; t < 64; t += blockDim.x) {
+        const int m = t / 8, p = t % 8;
+        s_leg[t] = m < 8 ? leg_scale(m) * leg_coef(m, p) : 0.0;
+    }
+    for (int t = threadIdx.x; t < 8; t += blockDim.x) {
+        s_bon[t] = bonnet_a(t);
+        s_bon[8 + t] = bonnet_b(t);
+    }
+    for (int t = lane; t < SM::X; t += 32) X[t] = 0.0;
+    for (int t = lane; t < NRHS; t += 32) rhs[t] = 0.0;
+    for (int t = lane; t < kNearBlock; t += 32) blk[t] = 0.f;
+    __syncthreads();
+
+    double afrag[KSMAX];
+#pragma unroll
+    for (int s = 0; s < KSMAX; ++s) afrag[s] = s_wP[(lane >> 2) * kMaxLQ + 4 * s + (lane & 3)];
+
+    const int i = blockIdx.x;
+    const double xi[3] = {a.pos[3 * i], a.pos[3 * i + 1], a.pos[3 * i + 2]};
+    const double t[3] = {a.ori[3 * i], a.ori[3 * i + 1], a.ori[3 * i + 2]};
+    const double e2 = 2.0 * tab.eps2, e6 = 6.0 * tab.eps2;
+    const double D1 = tab.D1, sv = 0.5 / tab.d, sw = 1.5 / tab.d;
+    const double *f = tab.half_force;
+    const int cnt = a.near_cnt[i];
+    const int *list = a.near_list + (int64_t)i * a.M;
+    const int slot0 = a.near_off[i];
+
+    for (int sidx = warp; sidx < cnt; sidx += kNearWarps) {
+        const int j = list[sidx];
+        const double D[3] = {xi[0] - a.pos[3 * j], xi[1] - a.pos[3 * j + 1], xi[2] - a.pos[3 * j + 2]};
+        const double p[3] = {a.ori[3 * j], a.ori[3 * j + 1], a.ori[3 * j + 2]};
+        // per-point scalars u_p (cols 0..N), v_p (cols N+1..2N+3)
+        for (int q = lane; q < LQ; q += 32) {
+            const double sq = s_pv[q];
+            const double r0x = D[0] + sq * t[0], r0y = D[1] + sq * t[1], r0z = D[2] + sq * t[2];
+            const double b = -2.0 * (p[0] * r0x + p[1] * r0y + p[2] * r0z);
+            const double c = r0x * r0x + r0y * r0y + r0z * r0z;
+            double I[SD::KW], J[SD::KW], S[SD::KW];
+            moments_near<N>(b, c, I, J, S);
+#pragma unroll
+            for (int pp = 0; pp < NL; ++pp) X[pp * kXq + q] = I[pp] + e2 * J[pp];
+#pragma unroll
+            for (int pp = 0; pp < NV; ++pp) X[(NL + pp) * kXq + q] = J[pp] - e6 * S[pp];
+        }
+        __syncwarp();
+        // projections Tm[k][col] = sum_q w_q P_k(s_q) X[col][q] on the FP64 tensor cores
+#pragma unroll
+        for (int tile = 0; tile < 2; ++tile) {
+            double d0 = 0.0, d1 = 0.0;
+#pragma unroll
+            for (int s = 0; s < KSMAX; ++s)
+                if (s < KS) {
+                    const double bf = X[(8 * tile + (lane >> 2)) * kXq + 4 * s + (lane & 3)];
+                    dmma_8x8x4(d0, d1, afrag[s], bf, d0, d1);
+                }
+            Tm[(lane >> 2) * 16 + 8 * tile + 2 * (lane & 3)] = d0;
+            Tm[(lane >> 2) * 16 + 8 * tile + 2 * (lane & 3) + 1] = d1;
+        }
+        __syncwarp();
+        PairTensors<double> P;
+        P.set(D, t, p);
+        for (int u = lane; u < NL * NL; u += 32) {
+            const int m = u / NL, k = u - m * NL;
+            const double *lg = s_leg + m * 8;
+            // coefficient sets of weight m at rows k-2..k+2
+            double AI = 0.0, E = 0.0, R0[5] = {0, 0, 0, 0, 0}, C0[3] = {0, 0, 0};
+            for (int pp = m; pp >= 0; pp -= 2) {
+                const double c = lg[pp];
+                AI += c * Tm[k * 16 + pp];
+                E += c * Tm[k * 16 + NL + pp + 2];
+#pragma unroll
+                for (int o = 0; o < 5; ++o) {
+                    const int kk = k - 2 + o;
+                    if (kk >= 0) R0[o] += c * Tm[kk * 16 + NL + pp];
+                }
+#pragma unroll
+                for (int o = 0; o < 3; ++o) {
+                    const int kk = k - 1 + o;
+                    if (kk >= 0) C0[o] -= c * Tm[kk * 16 + NL + pp + 1];
+                }
+            }
+            const double *al = s_bon, *be = s_bon + 8;
+            const double R1p = al[k + 1] * R0[4] + be[k + 1] * R0[2];                // R1_{k+1}
+            const double R1m = k > 0 ? al[k - 1] * R0[2] + be[k - 1] * R0[0] : 0.0;  // R1_{k-1}
+            const double R1 = al[k] * R0[3] + be[k] * R0[1];
+            const double R2 = al[k] * R1p + be[k] * R1m;
+            const double C1 = al[k] * C0[2] + be[k] * C0[0];
+            double th[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                th[c] = (c < 3 ? AI : 0.0) + R0[2] * P.DD[c] + R1 * P.DT[c] + R2 * P.TT[c] + C0[1] * P.PD[c] +
+                        C1 * P.PT[c] + E * P.PP[c];
+            if (m == 0) {
+                rhs[3 * k + 0] += th[0] * f[0] + th[3] * f[1] + th[4] * f[2];
+                rhs[3 * k + 1] += th[3] * f[0] + th[1] * f[1] + th[5] * f[2];
+                rhs[3 * k + 2] += th[4] * f[0] + th[5] * f[1] + th[2] * f[2];
+                continue;
+            }
+            double Q[3];
+#pragma unroll
+            for (int bb = 0; bb < 3; ++bb)
+                Q[bb] = th[sym_index(bb, 0)] * t[0] + th[sym_index(bb, 1)] * t[1] + th[sym_index(bb, 2)] * t[2];
+            if (k >= 1) {
+                const double gk = tab.gamma[k], ek = tab.Ek[k];
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa)
+                        blk[(m - 1) * kNearWeight + bb * RB + 3 * (k - 1) + aa] =
+                            (float)((k == 1) ? D1 * t[aa] * Q[bb] : gk * (th[sym_index(aa, bb)] - ek * t[aa] * Q[bb]));
+            }
+            if (PANELS && k <= 1) {
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa)
+                        blk[(m - 1) * kNearWeight + 3 * RB + k * 9 + bb * 3 + aa] = (float)(
+                            (k == 0) ? sv * th[sym_index(aa, bb)] : sw * (th[sym_index(aa, bb)] - Q[bb] * t[aa]));
+            }
+        }
+        __syncwarp();
+        if (!DIRECT) {
+            float4 *dst = reinterpret_cast<float4 *>(a.nearbuf + (int64_t)(slot0 + sidx) * kNearBlock);
+            const float4 *src = reinterpret_cast<const float4 *>(blk);
+            for (int e = lane; e < kNearBlock / 4; e += 32) dst[e] = src[e];
+        } else {
+            for (int e = lane; e < N * kNearWeight; e += 32) {
+                const int mm = e / kNearWeight, r = e - mm * kNearWeight;
+                const float v = blk[e];
+                if (r < 3 * RB) {
+                    const int col = 3 * mm + r / RB, rr = r % RB;
+                    const int64_t idx = ((int64_t)j * RB + col) * a.lda + (int64_t)i * RB + rr;
+                    if (a.A32) a.A32[idx] = v;
+                    if (a.A16) a.A16[idx] = __float2bfloat16_rn(v);
+                } else if (PANELS && r < 3 * RB + 18) {
+                    const int e2 = r - 3 * RB, w = e2 / 9, rem = e2 - w * 9, bb = rem / 3, aa = rem - bb * 3;
+                    (w ? a.PW32 : a.PV32)[((int64_t)j * RB + 3 * mm + bb) * a.ldp + (int64_t)i * 3 + aa] = v;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < NRHS; r += blockDim.x) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kNearWarps; ++w) s += s_wP[SM::TABLES + (size_t)w * SM::WARP + SM::X + SM::TM + SM::BLK + r];
+        a.near_contr[(int64_t)i * NRHS + r] = s;
+    }
+}
+
+// ---------------------------------------------------------------- finish
+// b rows and the l = 0 velocity terms from the summed theta^k_0 f
+// (matrix_assembly.f90:874-899; coeffs_and_vels.f90:698-705 for the velocity).
+__global__ void split_finish_kernel(SplitArgs a, int nchunks, double *b, double *vpart) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.M) return;
+    const int N = a.N, NRHS = 3 * (N + 1);
+    const Tables &tab = *a.tab;
+    const double *t = a.ori + 3 * i;
+    for (int k = 0; k <= N; ++k) {
+        double contr[3];
+        for (int c = 0; c < 3; ++c) {
+            double s = 0.0;
+            for (int ch = 0; ch < nchunks; ++ch) s += a.far_contr[((int64_t)ch * a.M + i) * NRHS + 3 * k + c];
+            if (a.near_contr) s += a.near_contr[(int64_t)i * NRHS + 3 * k + c];
+            contr[c] = s;
+        }
+        const double tdc = t[0] * contr[0] + t[1] * contr[1] + t[2] * contr[2];
+        for (int aa = 0; aa < 3; ++aa) {
+            if (k >= 1) {
+                const double v = (k == 1) ? -tab.D1 * tdc * t[aa] : -tab.gamma[k] * (contr[aa] - tab.Ek[k] * tdc * t[aa]);
+                b[(int64_t)i * 3 * N + 3 * (k - 1) + aa] = v;
+            }
+            if (vpart && k == 0) vpart[(int64_t)i * 6 + aa] = 0.5 / tab.d * contr[aa];
+            if (vpart && k == 1) vpart[(int64_t)i * 6 + 3 + aa] = 1.5 / tab.d * (contr[aa] - tdc * t[aa]);
+        }
+    }
+}
+
+template <int N, bool PANELS, bool FAR>
+cudaError_t launch_far_n(const SplitArgs &a, int far_chunks, cudaStream_t st) {
+    const size_t smem = FarSmem<N, PANELS>::bytes();
+    auto kern = far_pairs_kernel<N, PANELS, FAR>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    dim3 grid((a.M + 31) / 32, far_chunks);
+    kern<<<grid, 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int N, bool PANELS, bool DIRECT>
+cudaError_t launch_near_n(const SplitArgs &a, cudaStream_t st) {
+    const size_t smem = NearSmem<N>::bytes();
+    auto kern = near_pairs_kernel<N, PANELS, DIRECT>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return err;
+    kern<<<a.M, kNearWarps * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// N <= 5: the near kernel projects onto P_0..P_{N+2} with one 8-row tensor-core tile
+bool split_supported(int N, int LQ) { return N >= 1 && N <= 5 && LQ <= kMaxLQ; }
+
+int split_far_chunks(int M, int sm_count) {
+    const int groups = (M + 31) / 32;
+    const int target = sm_count * 8 * 8;  // about eight waves of resident one-warp CTAs
+    int chunks = (target + groups - 1) / groups;
+    return std::max(1, std::min(chunks, M));
+}
+
+cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st) {
+    cudaError_t err = cudaMemsetAsync(a.near_total, 0, sizeof(int), st);
+    if (err != cudaSuccess) return err;
+    classify_kernel<<<(a.M + kClassifyWarps - 1) / kClassifyWarps, kClassifyWarps * 32, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_far(const SplitArgs &a, int far_chunks, cudaStream_t st) {
+    const bool panels = a.PV32 != nullptr;
+    // far pairs have c >= near_c and d >= c * axis_ratio: with the defaults
+    // (near_c >= 10, axis_ratio >= 1e-6) only the backward recursion and the
+    // regular closed forms can occur
+    const bool far_only = a.near_bits != nullptr && a.near_c >= 10.0 && a.axis_ratio >= 1e-6;
+    switch (a.N) {
+#define RF_FAR_CASE(n)                                                                                     \
+    case n:                                                                                                \
+        if (panels) return far_only ? launch_far_n<n, true, true>(a, far_chunks, st)                       \
+                                    : launch_far_n<n, true, false>(a, far_chunks, st);                     \
+        return far_only ? launch_far_n<n, false, true>(a, far_chunks, st)                                  \
+                        : launch_far_n<n, false, false>(a, far_chunks, st);
+        RF_FAR_CASE(1)
+        RF_FAR_CASE(2)
+        RF_FAR_CASE(3)
+        RF_FAR_CASE(4)
+        RF_FAR_CASE(5)
+#undef RF_FAR_CASE
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_split_near(const SplitArgs &a, bool direct, cudaStream_t st) {
+    const bool panels = a.PV32 != nullptr;
+    switch (a.N) {
+#define RF_NEAR_CASE(n)                                                                                    \
+    case n:                                                                                                \
+        if (panels) return direct ? launch_near_n<n, true, true>(a, st) : launch_near_n<n, true, false>(a, st); \
+        return direct ? launch_near_n<n, false, true>(a, st) : launch_near_n<n, false, false>(a, st);
+        RF_NEAR_CASE(1)
+        RF_NEAR_CASE(2)
+        RF_NEAR_CASE(3)
+        RF_NEAR_CASE(4)
+        RF_NEAR_CASE(5)
+#undef RF_NEAR_CASE
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_split_finish(const SplitArgs &a, int far_chunks, double *b, double *vpart, cudaStream_t st) {
+    split_finish_kernel<<<(a.M + 127) / 128, 128, 0, st>>>(a, far_chunks, b, vpart);
+    return cudaGetLastError();
+}
+
+}  // namespace rf

@@ -48,6 +48,17 @@ struct rf_handle {
     double *PV64 = nullptr, *PW64 = nullptr;
     float *PV32 = nullptr, *PW32 = nullptr;
     double *vpart = nullptr;   // [asm_chunks][6M]
+    int vpart_chunks = 1;      // partial sums held in vpart by the last assembly
+    // split mixed-precision assembly
+    bool split = false;
+    int far_chunks = 1, far_chunk = 1;
+    uint32_t *near_bits = nullptr;
+    int *near_list = nullptr, *near_cnt = nullptr, *near_pref = nullptr, *near_off = nullptr;
+    int *near_total = nullptr;
+    float *nearbuf = nullptr;
+    int64_t near_cap = 0;      // capacity of nearbuf in pairs
+    int64_t near_pairs = 0;    // near pairs of the last assembly
+    double *far_contr = nullptr, *near_contr = nullptr;
     double *pvx = nullptr, *pwx = nullptr;
     // matvec workspace
     double *work64 = nullptr;

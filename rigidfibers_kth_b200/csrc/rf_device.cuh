@@ -137,7 +137,10 @@ __device__ __forceinline__ void moments_fp64(double b, double c, double *I, doub
 // cancellation te/ue - tb/ub (which loses all FP32 digits when the target
 // point lies near the source axis): te/ue - tb/ub = 2b d / ((te ub + tb ue) ue ub)
 // when te and tb share a sign.  Callers route points with d < c/16 to FP64.
-template <int N>
+// FAR = true: the caller guarantees c >= 10 and d >= 1e-6 c (far pairs of the
+// split assembly), so only the regular closed forms and the backward recursion
+// are compiled.
+template <int N, bool FAR = false>
 __device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *J, float *S) {
     constexpr int K = N + 3;
     const float ue = sqrtf(1.0f + b + c);
@@ -151,7 +154,7 @@ __device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *
     const float ab = (tb >= 0.f) ? (tb + ub) : d * __frcp_rn(ub - tb);
     I[0] = logf(ae * __frcp_rn(ab));
     I[1] = ue - ub - 0.5f * b * I[0];
-    if (d < 1e-6f * c) {
+    if (!FAR && d < 1e-6f * c) {
         // point on the source axis: the d -> 0 limits (Int_analytical.f90:162-164, 189-191)
         J[0] = 0.5f * (__frcp_rn(tb * tb) - __frcp_rn(te * te));
         J[1] = -iue + iub - 0.5f * b * J[0];
@@ -170,7 +173,7 @@ __device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *
         S[1] = (-(b + 2.0f * c) * iue3 + (-b + 2.0f * c) * iub3) * (id * (1.0f / 6.0f)) -
                b * (1.0f / 3.0f) * id * J[0];
     }
-    if (c < 10.0f) {
+    if (!FAR && c < 10.0f) {
 #pragma unroll
         for (int n = 2; n < K; ++n) {
             const float nn = n + 1.0f;

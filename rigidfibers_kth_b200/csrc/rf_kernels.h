@@ -35,6 +35,43 @@ struct AsmArgs {
 };
 
 cudaError_t launch_assemble(const AsmArgs &a, bool numeric, int pmode, int nchunks, cudaStream_t st);
+
+// Mixed-precision assembly split into far pairs (FP32) and near pairs (FP64),
+// analytic integration, N <= 5 (assemble_split.cu).
+struct SplitArgs {
+    int M, N, LQ;
+    const double *pos, *ori;
+    const Tables *tab;
+    float *A32;                // FP32 matrix or null
+    __nv_bfloat16 *A16;        // BF16 matrix or null
+    int64_t lda;
+    float *PV32, *PW32;        // velocity panels or null
+    int64_t ldp;
+    uint32_t *near_bits;       // [M][words] near-pair bitmap; null: every pair is far
+    int words;                 // (M + 31) / 32
+    int *near_list;            // [M][M] near sources of each target, ascending
+    int *near_cnt;             // [M]
+    int *near_pref;            // [M][words] near sources before each bitmap word
+    int *near_off;             // [M] first slot of each target in the near-pair buffer
+    int *near_total;           // device counter of near pairs (slot allocator)
+    float *nearbuf;            // [near pairs][320] FP64-integrated blocks in FP32
+    int merge;                 // far kernel copies near blocks from nearbuf
+    double *far_contr;         // [far_chunks][M][3(N+1)] partial sums of theta^k_0 f
+    double *near_contr;        // [M][3(N+1)] or null
+    int chunk;                 // sources per far-pair CTA
+    double near_c;             // c below which a pair is near
+    double axis_ratio;         // d < c*axis_ratio makes a pair near
+};
+constexpr int kNearBlockFloats = 320;
+bool split_supported(int N, int LQ);
+int split_far_chunks(int M, int sm_count);
+cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st);
+// direct = false: blocks to nearbuf (before the far kernel, which merges them);
+// direct = true: blocks straight into A (after the far kernel)
+cudaError_t launch_split_near(const SplitArgs &a, bool direct, cudaStream_t st);
+cudaError_t launch_split_far(const SplitArgs &a, int far_chunks, cudaStream_t st);
+// writes b (n) and, when vpart is not null, the l = 0 velocity terms [6M]
+cudaError_t launch_split_finish(const SplitArgs &a, int far_chunks, double *b, double *vpart, cudaStream_t st);
 cudaError_t launch_reduce_chunks(const double *part, int nchunks, int64_t stride, int64_t len, double *out,
                                  cudaStream_t st);
 

@@ -234,11 +234,50 @@ def _fp64_reference(pos, ori, eps, tol=1e-12):
     return x, V, W
 
 
+def _split_layout(kind, M):
+    if kind == "cloud":  # the sedimenting-cloud density of the M=4000 benchmark: many near pairs
+        return rf.generate_layout(M, "gaussian", 3.0 * (M / 4000) ** (1 / 3), 0.2, seed=1700 + M)
+    return rf.generate_layout(M, "uniform", 5.0 * (M / 1000) ** (1 / 3), 0.2, seed=1800 + M)
+
+
+@pytest.mark.parametrize("kind", ["cloud", "uniform"])
+@pytest.mark.parametrize("prec", [rf.PREC_MIXED_BF16, rf.PREC_FP32])
+def test_split_assembly_matches_fp64_matrix(kind, prec):
+    """FP32 far pairs + FP64 near pairs against the FP64 system, M not a multiple of 32.
+
+    Entry-wise the FP32 storage alone rounds at 6e-8 of each entry; the bound is
+    on the largest deviation relative to the largest entry.  The plain FP32
+    method (PREC_FP32) integrates every pair in FP32, including the forward
+    recursion of the moments near the source fiber, which amplifies FP32
+    rounding by up to ~1e5 for nearly touching pairs; its bound only guards
+    against gross errors (its velocities are checked against FP64 below).
+    """
+    M = 333
+    pos, ori = _split_layout(kind, M)
+    with make_sim(pos, ori, slenderness=1e-3) as s64:
+        s64.assemble_system()
+        A64, b64 = s64.matrix(), s64.rhs()
+    with make_sim(pos, ori, slenderness=1e-3, precision=prec, velocity_mode=rf.VEL_REUSE) as s:
+        s.assemble_system()
+        A, b = s.matrix(), s.rhs()
+    tol = 1e-6 if prec == rf.PREC_MIXED_BF16 else 5e-2
+    err = np.abs(A - A64).max() / np.abs(A64).max()
+    assert err <= tol, err
+    eb = np.linalg.norm(b - b64) / np.linalg.norm(b64)
+    assert eb <= tol, eb
+
+
+@pytest.mark.parametrize("layout", ["uniform", "cloud"])
+@pytest.mark.parametrize("vmode", [rf.VEL_RECOMPUTE, rf.VEL_REUSE])
 @pytest.mark.parametrize("prec", [rf.PREC_MIXED_BF16, rf.PREC_MIXED_FP32])
-def test_mixed_precision_velocity_error(prec):
-    pos, ori = rf.generate_layout(400, "uniform", 5.0, 0.2, seed=1003)
+def test_mixed_precision_velocity_error(prec, vmode, layout):
+    if layout == "uniform":
+        pos, ori = rf.generate_layout(400, "uniform", 5.0, 0.2, seed=1003)
+    else:
+        pos, ori = _split_layout("cloud", 400)
     x64, V64, W64 = _fp64_reference(pos, ori, 1e-3)
-    with make_sim(pos, ori, slenderness=1e-3, precision=prec, gmres_tol=1e-10, gmres_max_iters=200) as sim:
+    with make_sim(pos, ori, slenderness=1e-3, precision=prec, gmres_tol=1e-10, gmres_max_iters=200,
+                  velocity_mode=vmode) as sim:
         sim.assemble_system()
         assert sim.solve_system() == 0
         st = sim.solve_stats()
