@@ -44,6 +44,10 @@ WORKLOAD = dict(M=4000, distribution="gaussian", box=3.0, min_dist=0.2, seed=100
 # the one the same GMRES takes on it, from the FP64 run of this benchmark).
 FP64_MATVECS_PER_STEP = 26
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes (read + write) per stored element of A of one BF16 product, from
+# the ncu capture summarised in profiles/gemv_bf16_m1000.md; scaled to the
+# workload's matrix size (the traffic grows with the elements streamed)
+TRAFFIC_PER_ELEMENT = None
 
 
 def parse_args():
@@ -233,6 +237,7 @@ def run_ours(args):
     barrier(world)
     clocks.start()
     launches0 = sim.kernel_launches()
+    sim.gemv_timer(True)   # events around every inner-solve product of the timed region
     sim.mark(0)
     stats = []
     for _ in range(args.steps):
@@ -241,6 +246,7 @@ def run_ours(args):
         t += 1
     sim.mark(1)
     ms = sim.elapsed_ms(0, 1)
+    gemv_count, gemv_ms, gemv_bytes = sim.gemv_timer(False)
     launches = sim.kernel_launches() - launches0
     clk = clocks.stop()
     barrier(world)
@@ -297,21 +303,22 @@ def run_ours(args):
             verr = {"translational": float(np.abs(V - V64).max() / np.abs(V64).max()),
                     "rotational": float(np.abs(W - W64).max() / np.abs(W64).max()),
                     "bound": 1e-6, "norm": "max over fibers / max |FP64 velocity|"}
-        # roofline of the dominant kernel
-        solve_share = phases["solve"]
-        if phases["assemble"] >= solve_share:
-            dominant = "assemble_kernel"
-        else:
-            dominant = "gemv_partial_kernel (BF16 A, inner GMRES)"
+        # roofline of the dominant kernel: the inner-solve product (BF16 A), timed
+        # live over the timed region with events on the handle's stream
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
             os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        per_launch = gemv_ms / max(1, gemv_count)
+        achieved = gemv_bytes / (per_launch * 1e-3) / 1e9 if gemv_count else None
+        n_el = float(sim.matrix_ld()) * 3 * WORKLOAD["N"] * M
         roof = {"bound": "hbm", "kernel": "gemv_partial_kernel + gemv_reduce_kernel (BF16 A x FP32 x)",
-                "achieved": mv_bytes / (mv_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                "frac": mv_bytes / (mv_ms * 1e-3) / 1e9 / hbm_peak,
-                "traffic": None, "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                "algorithmic_bytes": mv_bytes, "ms_per_launch": mv_ms,
-                "dominant_phase": dominant}
+                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak if achieved else None,
+                "traffic": TRAFFIC_PER_ELEMENT * n_el if TRAFFIC_PER_ELEMENT else None,
+                "peak_source": "measured (copy)" if "hbm_gbs" in peaks else "fallback",
+                "algorithmic_bytes": gemv_bytes, "ms_per_launch": per_launch, "launches_timed": gemv_count,
+                "share_of_timed_region": gemv_ms / ms,
+                "isolated_ms_per_launch": mv_ms}
         cpu = None if args.no_cpu else cpu_baseline_sample(pos, ori, FP64_MATVECS_PER_STEP)
         n = 3 * WORKLOAD["N"] * M
         out = {

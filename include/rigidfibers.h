@@ -96,7 +96,7 @@ typedef struct rf_params {
     int32_t device;                      /* CUDA device ordinal */
     int32_t max_refinements;             /* mixed precision: outer refinement steps (default 30) */
     int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 12) */
-    double inner_tol;                    /* mixed precision: inner GMRES relative tolerance (default 1e-3) */
+    double inner_tol;                    /* mixed precision: inner GMRES relative tolerance (default 3e-3) */
     double near_field_c;                 /* mixed precision: squared distance below which the analytic
                                             integral stays FP64 (default 10, the recursion switch);
                                             >= 1e30 keeps every integral in FP64 */
@@ -179,6 +179,14 @@ double rf_timer_elapsed_ms(rf_handle *h, int32_t from, int32_t to);
  * the precision the inner GMRES uses (FP64, FP32 or BF16), over reps launches
  * on device-resident vectors; bytes of A streamed per product in *bytes. */
 rf_status rf_profile_matvec(rf_handle *h, int32_t reps, double *ms_per_product, double *bytes);
+/* Live timing of the inner-solve matrix-vector products (instrumentation; no
+ * counterpart in the reference).  enable = 1 resets the counters and brackets
+ * every following product of the inner GMRES (mixed and FP32 paths; the FP64
+ * GMRES otherwise) with events on the handle's stream; enable = 0 stops.
+ * Either way *count, *total_ms and *bytes_per_product report the products
+ * timed since the last reset, their summed device time and the bytes of A one
+ * product streams.  Pointers may be NULL. */
+rf_status rf_gemv_timer(rf_handle *h, int32_t enable, int64_t *count, double *total_ms, double *bytes_per_product);
 
 /* Sizes. */
 int64_t rf_system_size(const rf_handle *h);   /* n = 3*N*M */

@@ -128,6 +128,7 @@ def lib():
         "rf_timer_mark": (ctypes.c_int, [_h, ctypes.c_int32]),
         "rf_timer_elapsed_ms": (ctypes.c_double, [_h, ctypes.c_int32, ctypes.c_int32]),
         "rf_profile_matvec": (ctypes.c_int, [_h, ctypes.c_int32, _dp, _dp]),
+        "rf_gemv_timer": (ctypes.c_int, [_h, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), _dp, _dp]),
         "rf_system_size": (ctypes.c_int64, [_h]),
         "rf_matrix_ld": (ctypes.c_int64, [_h]),
         "rf_get_stream": (ctypes.c_void_p, [_h]),

@@ -41,6 +41,8 @@ void free_all(rf_handle *h) {
     if (h->hscal) cudaFreeHost(h->hscal);
     for (auto &ev : h->marks)
         if (ev) cudaEventDestroy(ev);
+    for (auto &ev : h->gt.ev)
+        if (ev) cudaEventDestroy(ev);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -146,6 +148,50 @@ rf_status cuda_fail(rf_handle *h, cudaError_t e, const char *what) {
 
 }  // namespace rf
 
+namespace {
+
+// Sum the recorded start/stop pairs of the product timer (waits for them).
+cudaError_t gemv_timer_flush(rf_handle *h) {
+    auto &g = h->gt;
+    if (g.used == 0) return cudaSuccess;
+    cudaError_t e = cudaEventSynchronize(g.ev[g.used - 1]);
+    for (int i = 0; i + 1 < g.used && e == cudaSuccess; i += 2) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, g.ev[i], g.ev[i + 1]);
+        g.total_ms += ms;
+        g.count++;
+    }
+    g.used = 0;
+    return e;
+}
+
+// Run one inner-solve product, bracketed by events when the timer is on.
+template <typename F>
+cudaError_t timed_product(rf_handle *h, double bytes, F launch) {
+    auto &g = h->gt;
+    if (!g.on) return launch();
+    if (g.used + 2 > (int)g.ev.size()) {
+        cudaError_t e = gemv_timer_flush(h);
+        if (e != cudaSuccess) return e;
+        while ((int)g.ev.size() < 64) {
+            cudaEvent_t ev = nullptr;
+            e = cudaEventCreate(&ev);
+            if (e != cudaSuccess) return e;
+            g.ev.push_back(ev);
+        }
+    }
+    cudaError_t e = cudaEventRecord(g.ev[g.used], h->stream);
+    if (e == cudaSuccess) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(g.ev[g.used + 1], h->stream);
+    if (e == cudaSuccess) {
+        g.used += 2;
+        g.bytes = bytes;
+    }
+    return e;
+}
+
+}  // namespace
+
 extern "C" {
 
 void rf_params_default(rf_params *p) {
@@ -170,7 +216,7 @@ void rf_params_default(rf_params *p) {
     p->device = 0;
     p->max_refinements = 30;
     p->cluster_size = 12;
-    p->inner_tol = 1e-3;
+    p->inner_tol = 3e-3;
     p->near_field_c = 10.0;
 }
 
@@ -505,6 +551,21 @@ rf_status rf_assemble_system(rf_handle *h) {
     return RF_OK;
 }
 
+rf_status rf_gemv_timer(rf_handle *h, int32_t enable, int64_t *count, double *total_ms, double *bytes_per_product) {
+    if (!h) return RF_ERR_INVALID_ARG;
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    CK(h, gemv_timer_flush(h), "product timer");
+    if (count) *count = h->gt.count;
+    if (total_ms) *total_ms = h->gt.total_ms;
+    if (bytes_per_product) *bytes_per_product = h->gt.bytes;
+    if (enable) {
+        h->gt.count = 0;
+        h->gt.total_ms = 0.0;
+    }
+    h->gt.on = enable != 0;
+    return RF_OK;
+}
+
 rf_status rf_solve_system(rf_handle *h) {
     if (!h) return RF_ERR_INVALID_ARG;
     if (!h->assembled) return rf::fail(h, RF_ERR_INVALID_ARG, "solve_system before assemble_system");
@@ -523,8 +584,11 @@ rf_status rf_solve_system(rf_handle *h) {
     if (prec == RF_PREC_FP64) {
         rf::Gmres<double>::Op A = [h](const double *in, double *out) {
             h->launches += 2;
-            return rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, in, out, nullptr,
-                                                                   h->work64, h->work_elems, h->sm_count, h->stream);
+            return timed_product(h, 8.0 * h->lda * h->n, [&] {
+                return rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, in, out, nullptr,
+                                                                       h->work64, h->work_elems, h->sm_count,
+                                                                       h->stream);
+            });
         };
         rf::Gmres<double>::Op P = [h, nb](const double *in, double *out) {
             return rf::launch_block_apply<double>(h->M, nb, h->Pblocks, in, out, h->stream);
@@ -539,8 +603,10 @@ rf_status rf_solve_system(rf_handle *h) {
     } else if (prec == RF_PREC_FP32) {
         rf::Gmres<float>::Op A = [h](const float *in, float *out) {
             h->launches += 2;
-            return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
-                                                               h->work32, h->work_elems, h->sm_count, h->stream);
+            return timed_product(h, 4.0 * h->lda * h->n, [&] {
+                return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
+                                                                   h->work32, h->work_elems, h->sm_count, h->stream);
+            });
         };
         rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
             return rf::launch_block_apply<float>(h->M, nb, h->Pblocks, in, out, h->stream);
@@ -564,12 +630,14 @@ rf_status rf_solve_system(rf_handle *h) {
         const bool bf16 = prec == RF_PREC_MIXED_BF16;
         rf::Gmres<float>::Op Alo = [h, bf16](const float *in, float *out) {
             h->launches += 2;
-            if (bf16)
-                return rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, h->n, h->n, in, out,
-                                                                           nullptr, h->work32, h->work_elems,
-                                                                           h->sm_count, h->stream);
-            return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
-                                                               h->work32, h->work_elems, h->sm_count, h->stream);
+            return timed_product(h, (bf16 ? 2.0 : 4.0) * h->lda * h->n, [&] {
+                if (bf16)
+                    return rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, h->n, h->n, in, out,
+                                                                               nullptr, h->work32, h->work_elems,
+                                                                               h->sm_count, h->stream);
+                return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
+                                                                   h->work32, h->work_elems, h->sm_count, h->stream);
+            });
         };
         rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
             return rf::launch_block_apply<float>(h->M, nb, h->Pblocks, in, out, h->stream);
@@ -600,7 +668,7 @@ rf_status rf_solve_system(rf_handle *h) {
             return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
         int it = 0, iters = 0;
         const int max_ref = h->p.max_refinements > 0 ? h->p.max_refinements : 30;
-        const double itol = h->p.inner_tol > 0.0 ? h->p.inner_tol : 1e-3;
+        const double itol = h->p.inner_tol > 0.0 ? h->p.inner_tol : 3e-3;
         while (e == cudaSuccess && bn > 0.0 && rn / bn > tol && it < max_ref && iters < maxit * max_ref) {
             // d = argmin |r/rn - A_lo d|, then x += rn * d
             e = rf::launch_scale_h<float, double>(h->n, h->r64, 1.0 / rn, h->r32, st);
@@ -608,7 +676,7 @@ rf_status rf_solve_system(rf_handle *h) {
             h->launches++;
             e = cudaMemsetAsync(h->d32, 0, sizeof(float) * h->n, st);
             if (e != cudaSuccess) break;
-            e = h->gm32->solve(Alo, use_pc ? &P : nullptr, h->r32, h->d32, true, itol, maxit, &res);
+            e = h->gm32->solve(Alo, use_pc ? &P : nullptr, h->r32, h->d32, true, itol, maxit, &res, false);
             if (e != cudaSuccess) break;
             if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
             h->launches += res.launches;

@@ -126,7 +126,7 @@ cudaError_t Gmres<VT>::update_solution(const Op *P, const VT *x, int k, VT *xcur
 
 template <typename VT>
 cudaError_t Gmres<VT>::solve(const Op &A, const Op *P, const VT *b, VT *x, bool x_is_zero, double tol,
-                             int max_iters, GmresResult *res) {
+                             int max_iters, GmresResult *res, bool check_true) {
     *res = GmresResult();
     const int m = m_;
     const int ld = m + 1;
@@ -214,6 +214,13 @@ cudaError_t Gmres<VT>::solve(const Op &A, const Op *P, const VT *b, VT *x, bool 
             res->iterations = itn;
             if (bea <= tol || itn >= iterMax) {
                 RF_TRY(update_solution(P, x, jH + 1, xcur_, res));
+                if (!check_true) {
+                    RF_TRY(cudaMemcpyAsync(x, xcur_, sizeof(VT) * n_, cudaMemcpyDeviceToDevice, st_));
+                    RF_TRY(cudaStreamSynchronize(st_));
+                    res->backward_error = bea;
+                    res->info = bea <= tol ? 0 : -4;
+                    return cudaSuccess;
+                }
                 RF_TRY(residual(A, b, xcur_, w_, res));
                 double tn;
                 RF_TRY(launch_dot<VT>(n_, w_, w_, hcol_ + m + 5, rb_, st_));

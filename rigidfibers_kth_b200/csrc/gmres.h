@@ -37,9 +37,11 @@ class Gmres {
     ~Gmres();
     cudaError_t init(int64_t n, int m, cudaStream_t st);
     // Solve A x = b; x holds the initial guess (device, VT).  If x_is_zero the
-    // initial residual is b itself (no matvec, like icntl(6) = 0).
+    // initial residual is b itself (no matvec, like icntl(6) = 0).  With
+    // check_true = false the solve stops on the Arnoldi estimate alone (inner
+    // solves of iterative refinement, whose caller recomputes the residual).
     cudaError_t solve(const Op &A, const Op *P, const VT *b, VT *x, bool x_is_zero, double tol, int max_iters,
-                      GmresResult *res);
+                      GmresResult *res, bool check_true = true);
     int restart() const { return m_; }
 
    private:

@@ -6,6 +6,7 @@
 
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../../include/rigidfibers.h"
 #include "gmres.h"
@@ -82,6 +83,16 @@ struct rf_handle {
     bool mlp_loaded = false;
     float *feat = nullptr;     // M x 144 features
     float *mlp_h1 = nullptr, *mlp_h2 = nullptr, *mlp_out = nullptr;
+
+    // live timing of the inner-solve products (rf_gemv_timer)
+    struct GemvTimer {
+        bool on = false;
+        std::vector<cudaEvent_t> ev;   // start/stop pairs
+        int used = 0;
+        int64_t count = 0;
+        double total_ms = 0.0;
+        double bytes = 0.0;
+    } gt;
 
     rf_solve_stats stats{};
     bool assembled = false;

@@ -15,6 +15,8 @@
 // Reductions.  Dot products and norms use one pass with a per-block partial,
 // and the last block to finish (ticket counter, no spinning) adds the
 // partials in block order and writes the scalar to device memory.
+#include <algorithm>
+
 #include "rf_kernels.h"
 
 namespace rf {
@@ -119,23 +121,51 @@ __global__ void gemv_reduce_kernel(const ACC *__restrict__ work, int splits, int
     else y[i] = (Y)s;
 }
 
-int gemv_splits(int64_t m, int64_t k, int vec, int sm_count) {
+// Resident CTAs of one instance on the whole GPU (queried once per instance).
+template <typename S, typename X, typename ACC>
+int gemv_slots(int sm_count) {
+    static int occ = 0;
+    if (occ == 0) {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, gemv_partial_kernel<S, X, ACC>, kGemvThreads, 0) !=
+                cudaSuccess ||
+            o < 1)
+            o = 1;
+        occ = o;
+    }
+    return sm_count * occ;
+}
+
+// Column splits: about kWaves full waves of resident CTAs, so that the last,
+// partial wave costs little; at least 64 columns per split.
+constexpr int kWaves = 8;
+int gemv_splits(int64_t m, int64_t k, int vec, int slots) {
     const int64_t tiles = (m + (int64_t)kGemvThreads * vec - 1) / ((int64_t)kGemvThreads * vec);
-    const int64_t target = (int64_t)sm_count * 8;
-    int64_t splits = (target + tiles - 1) / tiles;
-    const int64_t max_by_cols = k / 256 > 0 ? k / 256 : 1;
+    int64_t splits = ((int64_t)kWaves * slots + tiles - 1) / tiles;
+    const int64_t max_by_cols = k / 64 > 0 ? k / 64 : 1;
     if (splits > max_by_cols) splits = max_by_cols;
     if (splits < 1) splits = 1;
     return (int)splits;
 }
 
+template <typename S, typename X, typename ACC>
+int64_t gemv_work_elems_of(int64_t m, int sm_count) {
+    constexpr int VEC = Vec16<S>::kVec;
+    const int64_t tiles = (m + (int64_t)kGemvThreads * VEC - 1) / ((int64_t)kGemvThreads * VEC);
+    const int64_t mpad = tiles * kGemvThreads * VEC;
+    return (int64_t)gemv_splits(m, m, VEC, gemv_slots<S, X, ACC>(sm_count)) * mpad;
+}
+
 }  // namespace
 
 int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes) {
-    const int vec = 16 / elem_bytes;
-    const int64_t tiles = (m + (int64_t)kGemvThreads * vec - 1) / ((int64_t)kGemvThreads * vec);
-    const int64_t mpad = tiles * kGemvThreads * vec;
-    return (int64_t)gemv_splits(m, m, vec, sm_count) * mpad;
+    // the largest split buffer over the instances that read elements of this size
+    if (elem_bytes == 8) return gemv_work_elems_of<double, double, double>(m, sm_count);
+    if (elem_bytes == 4)
+        return std::max(gemv_work_elems_of<float, double, double>(m, sm_count),
+                        gemv_work_elems_of<float, float, float>(m, sm_count));
+    return std::max(gemv_work_elems_of<__nv_bfloat16, float, float>(m, sm_count),
+                    gemv_work_elems_of<__nv_bfloat16, double, double>(m, sm_count));
 }
 
 template <typename S, typename X, typename ACC, typename Y>
@@ -144,7 +174,7 @@ cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *
     constexpr int VEC = Vec16<S>::kVec;
     const int64_t tiles = (lda + (int64_t)kGemvThreads * VEC - 1) / ((int64_t)kGemvThreads * VEC);
     const int64_t mpad = tiles * kGemvThreads * VEC;
-    int splits = gemv_splits(m, k, VEC, sm_count);
+    int splits = gemv_splits(m, k, VEC, gemv_slots<S, X, ACC>(sm_count));
     while (splits > 1 && (int64_t)splits * mpad > work_elems) --splits;
     if ((int64_t)splits * mpad > work_elems) return cudaErrorInvalidValue;
     const int64_t cps = (k + splits - 1) / splits;

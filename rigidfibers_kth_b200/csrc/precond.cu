@@ -35,33 +35,67 @@ constexpr int kOut = RF_MLP_OUT;      // 225
 constexpr int kNb = 15;               // block size the MLP is built for (N = 5)
 
 // ------------------------------------------------------------------ k-NN
-// One thread per fiber: the K nearest centres (excluding itself), sorted.
-__global__ void knn_kernel(int M, const double *__restrict__ pos, int K, int *__restrict__ knn) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
-    float bd[16];
-    int bi[16];
-    for (int r = 0; r < 16; ++r) {
+// One warp per fiber: every lane keeps the K nearest of its sources j = lane,
+// lane + 32, ... sorted in registers (unrolled compare-and-swap), then K rounds
+// of a warp arg-min over the lane heads merge them.  Order: distance, then the
+// lower source index (the order of a sequential scan with strict comparison).
+constexpr int kKnnWarps = 4;
+__global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(int M, const double *__restrict__ pos, int K,
+                                                             int *__restrict__ knn) {
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kKnnWarps + (threadIdx.x >> 5);
+    if (i >= M) return;  // whole warp
+    float bd[kK];
+    int bi[kK];
+#pragma unroll
+    for (int r = 0; r < kK; ++r) {
         bd[r] = 3.4e38f;
-        bi[r] = -1;
+        bi[r] = 0x7fffffff;
     }
     const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
-    for (int j = 0; j < M; ++j) {
+    for (int j = lane; j < M; j += 32) {
         if (j == i) continue;
         const float dx = (float)(__ldg(pos + 3 * j) - xi), dy = (float)(__ldg(pos + 3 * j + 1) - yi),
                     dz = (float)(__ldg(pos + 3 * j + 2) - zi);
-        const float d = dx * dx + dy * dy + dz * dz;
-        if (d >= bd[K - 1]) continue;
-        int r = K - 1;
-        while (r > 0 && bd[r - 1] > d) {
-            bd[r] = bd[r - 1];
-            bi[r] = bi[r - 1];
-            --r;
+        float d = dx * dx + dy * dy + dz * dz;
+        if (!(d < bd[kK - 1])) continue;
+        int jj = j;
+#pragma unroll
+        for (int r = 0; r < kK; ++r) {
+            if (d < bd[r]) {  // this lane's sources arrive in increasing j: ties keep the earlier one
+                const float td = bd[r];
+                const int ti = bi[r];
+                bd[r] = d;
+                bi[r] = jj;
+                d = td;
+                jj = ti;
+            }
         }
-        bd[r] = d;
-        bi[r] = j;
     }
-    for (int r = 0; r < K; ++r) knn[(int64_t)i * K + r] = bi[r];
+    for (int r = 0; r < K; ++r) {
+        // lexicographic arg-min of (distance, index) over the lane heads
+        float md = bd[0];
+        int mi = bi[0];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float od = __shfl_xor_sync(0xffffffffu, md, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, mi, o);
+            if (od < md || (od == md && oi < mi)) {
+                md = od;
+                mi = oi;
+            }
+        }
+        if (lane == 0) knn[(int64_t)i * K + r] = mi < M ? mi : -1;
+        if (bi[0] == mi && bd[0] == md) {  // the winning lane pops its head
+#pragma unroll
+            for (int q = 0; q < kK - 1; ++q) {
+                bd[q] = bd[q + 1];
+                bi[q] = bi[q + 1];
+            }
+            bd[kK - 1] = 3.4e38f;
+            bi[kK - 1] = 0x7fffffff;
+        }
+    }
 }
 
 // ------------------------------------------------------------------ cluster inverse
@@ -421,7 +455,7 @@ rf_status build_preconditioner(rf_handle *h) {
         if ((s = ck(cudaMalloc(&h->knn, sizeof(int) * (size_t)M * kmax), "alloc knn")) != RF_OK) return s;
     }
     const int K = std::min(kmax, M - 1);
-    knn_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, h->X[h->cur], K, h->knn);
+    knn_kernel<<<(M + kKnnWarps - 1) / kKnnWarps, kKnnWarps * 32, 0, st>>>(M, h->X[h->cur], K, h->knn);
     h->launches++;
     if ((s = ck(cudaGetLastError(), "knn")) != RF_OK) return s;
     if (h->p.preconditioner == RF_PC_CLUSTER) {
@@ -535,7 +569,7 @@ rf_status rf_compute_features(rf_handle *h, float *features) {
             cudaMalloc(&h->mlp_out, sizeof(float) * (size_t)M * kOut) != cudaSuccess)
             return fail(h, RF_ERR_OOM, "alloc");
     }
-    knn_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->X[h->cur], kK, h->knn);
+    knn_kernel<<<(M + kKnnWarps - 1) / kKnnWarps, kKnnWarps * 32, 0, h->stream>>>(M, h->X[h->cur], kK, h->knn);
     features_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->X[h->cur], h->T[h->cur], h->knn, h->feat,
                                                             h->feat + (size_t)M * kIn);
     h->launches += 2;

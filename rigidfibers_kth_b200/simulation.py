@@ -43,7 +43,7 @@ class FiberParams:
     device: int = 0
     max_refinements: int = 30
     cluster_size: int = 12
-    inner_tol: float = 1e-3
+    inner_tol: float = 3e-3
     near_field_c: float = 10.0
 
     def to_c(self):
@@ -290,6 +290,21 @@ class Simulation:
         ms, nbytes = ctypes.c_double(), ctypes.c_double()
         L.check(L.lib().rf_profile_matvec(self._h, reps, ctypes.byref(ms), ctypes.byref(nbytes)), self._h)
         return ms.value, nbytes.value
+
+    def system_size(self):
+        return L.lib().rf_system_size(self._h)
+
+    def matrix_ld(self):
+        """Leading dimension of the stored matrix (rows padded to 64)."""
+        return L.lib().rf_matrix_ld(self._h)
+
+    def gemv_timer(self, enable):
+        """Start (True, counters reset) or stop live timing of the inner-solve
+        products; returns (products timed, their total ms, bytes of A per product)."""
+        cnt, ms, nbytes = ctypes.c_int64(), ctypes.c_double(), ctypes.c_double()
+        L.check(L.lib().rf_gemv_timer(self._h, 1 if enable else 0, ctypes.byref(cnt), ctypes.byref(ms),
+                                      ctypes.byref(nbytes)), self._h)
+        return cnt.value, ms.value, nbytes.value
 
     def kernel_launches(self):
         return L.lib().rf_kernel_launches(self._h)

@@ -68,6 +68,21 @@ def test_features_and_targets_rotate_with_the_configuration():
     assert np.abs(t0 - t1).max() <= 1e-3 * np.abs(t0).max()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("M", [17, 700])
+def test_features_follow_the_nearest_neighbours(M):
+    """The first three features of neighbour r are its centre in the fiber's
+    frame: their norms are the 16 smallest centre distances, in order."""
+    pos, ori = rf.generate_layout(M, "gaussian", 1.5 * (M / 200) ** (1 / 3), 0.2, seed=1510 + M)
+    with rf.Simulation(rf.Configuration(rf.FiberParams(slenderness=1e-3), pos, ori)) as sim:
+        f = sim.features().reshape(M, 16, 9)
+    d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
+    np.fill_diagonal(d, np.inf)
+    want = np.sort(d, axis=1)[:, :16]
+    got = np.linalg.norm(f[:, :, :3], axis=-1)
+    assert np.abs(got - want).max() <= 1e-5 * want.max()
+
+
 def _solve(pos, ori, pc, weights=None, prec=rf.PREC_FP64, tol=1e-10, max_iters=600):
     p = rf.FiberParams(slenderness=1e-3, gmres_tol=tol, gmres_max_iters=max_iters, preconditioner=pc, precision=prec,
                        gmres_restart=10)
