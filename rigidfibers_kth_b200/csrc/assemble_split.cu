@@ -149,7 +149,7 @@ __device__ __forceinline__ void moments_near(double b, double c, double *I, doub
     const double tb = -1.0 + 0.5 * b;
     const double d = c - 0.25 * b * b;
     const double iue = 1.0 / ue, iub = 1.0 / ub;
-    I[0] = log(fabs(2.0 + b + 2.0 * ue)) - log(fabs(-2.0 + b + 2.0 * ub));
+    I[0] = log(fabs((2.0 + b + 2.0 * ue) / (-2.0 + b + 2.0 * ub)));
     I[1] = ue - ub - 0.5 * b * I[0];
     if (d < 1e-14) {
         const double e1 = 1.0 + 0.5 * b, e2 = -1.0 + 0.5 * b;
@@ -633,15 +633,18 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
 // ---------------------------------------------------------------- near pairs (FP64)
 constexpr int kNearWarps = 4;
 constexpr int kXq = 52;  // q stride of X[col][q]: 52 = 4 mod 16 makes the B fragments conflict-free
+constexpr int kTmLd = 17;  // row stride of the projections Tm[k][col] (odd: rows fall in different banks)
 
 template <int N>
 struct NearSmem {
     static constexpr int X = 16 * kXq;                  // per-point scalars [col][q], cols >= 2N+4 zero
-    static constexpr int TM = 8 * 16;                   // projections [k][col]
+    static constexpr int TM = 8 * kTmLd + (8 * kTmLd) % 2;  // projections [k][col] (even: keeps BLK 16-byte aligned)
     static constexpr int BLK = kNearBlock / 2;          // staged block + panels (floats)
     static constexpr int RHS = 3 * (N + 1) + 1;
     static constexpr int WARP = X + TM + BLK + RHS + ((X + TM + BLK + RHS) & 1);
-    static constexpr int TABLES = 8 * kMaxLQ + kMaxLQ + 64 + 16;   // w P, s, Legendre coefficients, Bonnet
+    static constexpr int TABLES = 8 * kMaxLQ + kMaxLQ + 72 + 16;   // w P, s, Legendre coefficients, Bonnet
+    // every per-warp region and the staged block (read as float4) start on 16 bytes
+    static_assert(X % 2 == 0 && (X + TM) % 2 == 0 && WARP % 2 == 0 && TABLES % 2 == 0, "16-byte alignment");
     static size_t bytes() { return sizeof(double) * (TABLES + (size_t)kNearWarps * WARP); }
 };
 
@@ -661,8 +664,8 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double *s_wP = reinterpret_cast<double *>(smem_raw);   // [8][kMaxLQ]
     double *s_pv = s_wP + 8 * kMaxLQ;
-    double *s_leg = s_pv + kMaxLQ;                          // [8][8]: sc_m a_mp
-    double *s_bon = s_leg + 64;                             // alpha_k (0..7), beta_k (8..15)
+    double *s_leg = s_pv + kMaxLQ;                          // [8][9]: sc_m a_mp (odd row stride)
+    double *s_bon = s_leg + 72;                             // alpha_k (0..7), beta_k (8..15)
     double *base = s_wP + SM::TABLES + (size_t)warp * SM::WARP;
     double *X = base;
     double *Tm = X + SM::X;
@@ -677,9 +680,9 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
         s_wP[t] = (k < SD::KW && q < LQ) ? tab.wv[q] * tab.P[k][q] : 0.0;
     }
     for (int t = threadIdx.x; t < kMaxLQ; t += blockDim.x) s_pv[t] = t < LQ ? tab.pv[t] : 0.0;
-    for (int t = threadIdx.x; t < 64; t += blockDim.x) {
-        const int m = t / 8, p = t % 8;
-        s_leg[t] = m < 8 ? leg_scale(m) * leg_coef(m, p) : 0.0;
+    for (int t = threadIdx.x; t < 72; t += blockDim.x) {
+        const int m = t / 9, p = t % 9;
+        s_leg[t] = p < 8 ? leg_scale(m) * leg_coef(m, p) : 0.0;
     }
     for (int t = threadIdx.x; t < 8; t += blockDim.x) {
         s_bon[t] = bonnet_a(t);
@@ -732,30 +735,30 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
                     const double bf = X[(8 * tile + (lane >> 2)) * kXq + 4 * s + (lane & 3)];
                     dmma_8x8x4(d0, d1, afrag[s], bf, d0, d1);
                 }
-            Tm[(lane >> 2) * 16 + 8 * tile + 2 * (lane & 3)] = d0;
-            Tm[(lane >> 2) * 16 + 8 * tile + 2 * (lane & 3) + 1] = d1;
+            Tm[(lane >> 2) * kTmLd + 8 * tile + 2 * (lane & 3)] = d0;
+            Tm[(lane >> 2) * kTmLd + 8 * tile + 2 * (lane & 3) + 1] = d1;
         }
         __syncwarp();
         PairTensors<double> P;
         P.set(D, t, p);
         for (int u = lane; u < NL * NL; u += 32) {
             const int m = u / NL, k = u - m * NL;
-            const double *lg = s_leg + m * 8;
+            const double *lg = s_leg + m * 9;
             // coefficient sets of weight m at rows k-2..k+2
             double AI = 0.0, E = 0.0, R0[5] = {0, 0, 0, 0, 0}, C0[3] = {0, 0, 0};
             for (int pp = m; pp >= 0; pp -= 2) {
                 const double c = lg[pp];
-                AI += c * Tm[k * 16 + pp];
-                E += c * Tm[k * 16 + NL + pp + 2];
+                AI += c * Tm[k * kTmLd + pp];
+                E += c * Tm[k * kTmLd + NL + pp + 2];
 #pragma unroll
                 for (int o = 0; o < 5; ++o) {
                     const int kk = k - 2 + o;
-                    if (kk >= 0) R0[o] += c * Tm[kk * 16 + NL + pp];
+                    if (kk >= 0) R0[o] += c * Tm[kk * kTmLd + NL + pp];
                 }
 #pragma unroll
                 for (int o = 0; o < 3; ++o) {
                     const int kk = k - 1 + o;
-                    if (kk >= 0) C0[o] -= c * Tm[kk * 16 + NL + pp + 1];
+                    if (kk >= 0) C0[o] -= c * Tm[kk * kTmLd + NL + pp + 1];
                 }
             }
             const double *al = s_bon, *be = s_bon + 8;
