@@ -211,10 +211,12 @@ rf_status rf_generate_layout(int32_t M, int32_t distribution, double box, double
  * any two fibers; a geometry diagnostic (the kernels are singular at 0). */
 double rf_min_segment_distance(int32_t M, const double *positions, const double *orientations);
 
-/* ---- Learned preconditioner ----------------------------------------------
- * MLP: k=16 nearest-neighbour features (relative centre, orientation of the
- * neighbour, orientation of the fiber: 16 x 9 floats) -> 256 -> 256 -> 225,
- * ReLU, predicting a correction to the identity preconditioner block.
+/* ---- Learned preconditioner (benchmark addition; no reference counterpart)
+ * MLP: features of the k=16 nearest neighbours in the fiber's own frame
+ * (e3 = its orientation, e1 toward the nearest neighbour): per neighbour the
+ * relative centre (3) and the six products u_a u_b of its orientation
+ * (sign-invariant), 16 x 9 floats -> 256 -> 256 -> 225, ReLU, predicting the
+ * fiber's 15 x 15 block minus the identity in that frame.
  * Weights are FP32, layer-major: W1[256x144] b1[256] W2[256x256] b2[256]
  * W3[225x256] b3[225] (row-major, out x in). */
 #define RF_MLP_K 16

@@ -93,3 +93,14 @@ def test_oracle_matvec_and_rows_consistent(golden):
     # the diagonal blocks are the identity (matrix_assembly.f90:489-492)
     for i in range(30):
         assert np.array_equal(A[i * 15 : (i + 1) * 15, i * 15 : (i + 1) * 15], np.eye(15))
+
+
+def test_flop_count_of_the_reference_assembly():
+    """oracle/count_flops.py: the counted work per ordered pair behind the
+    assembly roofline (two sqrt and two log per Gauss point and 24 points)."""
+    from oracle import count_flops
+
+    fwd, bwd = count_flops.pair_cost(4.0), count_flops.pair_cost(40.0)
+    assert fwd["sqrt"] == bwd["sqrt"] == 48 and fwd["log"] == bwd["log"] == 48
+    assert bwd["div"] > fwd["div"]  # the backward recursion divides by c at every one of its 26 steps
+    assert 2.5e4 < fwd["add"] + fwd["mul"] < bwd["add"] + bwd["mul"] < 4.0e4
