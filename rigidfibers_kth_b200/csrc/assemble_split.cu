@@ -339,6 +339,106 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
     }
 }
 
+// Coefficient sets of weight m (parity PAR) for rows k = 0..N, staged per
+// lane as [k][AI, R0, R1, R2, C0, C1, E][lane].
+template <int N, int PAR>
+__device__ __forceinline__ void far_sets(int m, const float (&U)[N + 1][N + 1], const float (&V)[N + 3][N + 3],
+                                         float *s_set, int lane) {
+    constexpr int NP = (N - PAR) / 2 + 1;  // p = PAR, PAR + 2, ... <= N
+    float cf[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) cf[i] = c_leg32[m][PAR + 2 * i];
+    float R0[N + 3], C0[N + 2], R1[N + 2];
+#pragma unroll
+    for (int k = 0; k < N + 3; ++k) {
+        float s1 = 0.f;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) s1 = fmaf(cf[i], V[PAR + 2 * i][k], s1);
+        R0[k] = s1;
+    }
+#pragma unroll
+    for (int k = 0; k < N + 2; ++k) {
+        float s1 = 0.f;
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+            if (k < vrows(N, PAR + 2 * i + 1)) s1 = fmaf(cf[i], V[PAR + 2 * i + 1][k], s1);
+        C0[k] = -s1;
+    }
+#pragma unroll
+    for (int k = 0; k < N + 2; ++k)
+        R1[k] = (float)bonnet_a(k) * R0[k + 1] + (k > 0 ? (float)bonnet_b(k) * R0[k > 0 ? k - 1 : 0] : 0.f);
+#pragma unroll
+    for (int k = 0; k <= N; ++k) {
+        float ai = 0.f, ee = 0.f;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            ai = fmaf(cf[i], U[PAR + 2 * i][k], ai);
+            ee = fmaf(cf[i], V[PAR + 2 * i + 2][k], ee);
+        }
+        float *o = s_set + k * 7 * 32 + lane;
+        o[0] = ai;
+        o[32] = R0[k];
+        o[64] = R1[k];
+        o[96] = (float)bonnet_a(k) * R1[k + 1] + (k > 0 ? (float)bonnet_b(k) * R1[k > 0 ? k - 1 : 0] : 0.f);
+        o[128] = C0[k];
+        o[160] = (float)bonnet_a(k) * C0[k + 1] + (k > 0 ? (float)bonnet_b(k) * C0[k > 0 ? k - 1 : 0] : 0.f);
+        o[192] = ee;
+    }
+}
+
+// X = R0 D + R1 t + C0 p, Y = R1 D + R2 t + C1 p, Z = C0 D + C1 t + E p
+__device__ __forceinline__ void far_xyz(const float *o, const float *D, const float *t, const float *p, float *X,
+                                        float *Y, float *Z) {
+    const float R0 = o[32], R1 = o[64], R2 = o[96], C0 = o[128], C1 = o[160], E = o[192];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        X[c] = R0 * D[c] + R1 * t[c] + C0 * p[c];
+        Y[c] = R1 * D[c] + R2 * t[c] + C1 * p[c];
+        Z[c] = C0 * D[c] + C1 * t[c] + E * p[c];
+    }
+}
+
+// FP32 moments of a far pair (c >= 10, d >= c/16 at every point): the regular
+// closed forms without cancellation (te/ue - tb/ub rewritten when te and tb
+// share a sign, the logarithm argument formed stably), the hardware reciprocal
+// square root and reciprocal, and the backward recursion from n = 27 with the
+// per-item factors 1/c, b/c, (ue -+ ub)/c taken out of the loop.
+template <int N>
+__device__ __forceinline__ void far_moments(float b, float c, float *I, float *J, float *S) {
+    constexpr int K = N + 3;
+    const float xe = 1.0f + b + c, xb = 1.0f - b + c;
+    const float iue = rsqrtf(xe), iub = rsqrtf(xb);
+    const float ue = xe * iue, ub = xb * iub;
+    const float te = 1.0f + 0.5f * b, tb = -1.0f + 0.5f * b;
+    const float d = c - 0.25f * b * b;
+    const float id = __fdividef(1.0f, d);
+    const float ae = (te >= 0.f) ? (te + ue) : __fdividef(d, ue - te);
+    const float ab = (tb >= 0.f) ? (tb + ub) : __fdividef(d, ub - tb);
+    I[0] = logf(__fdividef(ae, ab));
+    I[1] = ue - ub - 0.5f * b * I[0];
+    J[0] = (te * tb > 0.f) ? __fdividef(2.0f * b, (te * ub + tb * ue) * ue * ub) : (te * iue - tb * iub) * id;
+    J[1] = -iue + iub - 0.5f * b * J[0];
+    const float iue3 = iue * iue * iue, iub3 = iub * iub * iub;
+    S[0] = ((2.0f + b) * iue3 - (-2.0f + b) * iub3) * (id * (1.0f / 6.0f)) + (2.0f / 3.0f) * id * J[0];
+    S[1] = (-(b + 2.0f * c) * iue3 + (-b + 2.0f * c) * iub3) * (id * (1.0f / 6.0f)) - b * (1.0f / 3.0f) * id * J[0];
+    const float ic = __fdividef(1.0f, c);
+    const float icb = ic * b, icwp = ic * (ue - ub), icwm = ic * (ue + ub);
+    float i1 = 0.f, i2 = 0.f, j1 = 0.f, j2 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
+    for (int n = 27; n >= 2; --n) {
+        // I_n = a0/c (r2 (ue - sbp ub) + cb b I_{n+1} - I_{n+2})  (Int_analytical.f90:137-157)
+        const float a0 = (n + 2.0f) / (n + 1.0f);
+        const float r2 = 1.0f / (n + 2.0f);
+        const float cb = (1.0f - 2.0f * (n + 2.0f)) / (2.0f * (n + 2.0f));
+        const float icw = ((n + 1) % 2 == 0) ? icwp : icwm;
+        const float in = fmaf((a0 * cb) * icb, i1, fmaf(-a0 * ic, i2, (a0 * r2) * icw));
+        const float jn = fmaf(ic, in, fmaf(-icb, j1, -ic * j2));
+        const float sn = fmaf(ic, jn, fmaf(-icb, s1, -ic * s2));
+        if (n < K) { I[n] = in; J[n] = jn; S[n] = sn; }
+        i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
+    }
+}
+
 template <int N, bool PANELS, bool FAR>
 __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a) {
     using SD = SplitDims<N>;
@@ -397,6 +497,11 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
         xj[0] = __ldg(a.pos + 3 * j0); xj[1] = __ldg(a.pos + 3 * j0 + 1); xj[2] = __ldg(a.pos + 3 * j0 + 2);
         pj[0] = (float)__ldg(a.ori + 3 * j0); pj[1] = (float)__ldg(a.ori + 3 * j0 + 1); pj[2] = (float)__ldg(a.ori + 3 * j0 + 2);
     }
+    // staging offsets of this thread's entries in a near record: block entries
+    // e = lane and lane + 32 (e = 3 RB columns-major), panel entry lane < 18
+    const int moff0 = (lane / RB) * GR + lane % RB;
+    const int moff1 = ((lane + 32) / RB) * GR + (lane + 32) % RB;
+    const int poff = 3 * GR + ((lane / 9) * 3 + (lane % 9) / 3) * 96 + (lane % 9) % 3;  // s_pan follows s_stg
     unsigned word = 0u;
     int wpref = 0;
     for (int j = j0; j < j1; ++j) {
@@ -427,7 +532,7 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
         }
         __syncwarp();
         for (int u = lane; u < nnear * (kNearWeight / 4); u += 32) {
-            const int r = u / (kNearWeight / 4), c = u - r * (kNearWeight / 4);
+            const int r = u >> 4, c = u & 15;  // kNearWeight / 4 = 16 chunks per record
             cp_async16(s_nb + r * kNearWeight + 4 * c, a.nearbuf + (int64_t)s_ns[r] * kNearBlock + 4 * c);
         }
         cp_async_commit();
@@ -450,7 +555,8 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
                 const float b = -2.0f * (p[0] * r0x + p[1] * r0y + p[2] * r0z);
                 const float c = r0x * r0x + r0y * r0y + r0z * r0z;
                 float I[KW], J[KW], S[KW];
-                moments_fp32<N, FAR>(b, c, I, J, S);
+                if (FAR) far_moments<N>(b, c, I, J, S);
+                else moments_fp32<N, false>(b, c, I, J, S);
                 const float *w = s_w + q * KW;
                 float wk[KW];
 #pragma unroll
@@ -509,114 +615,88 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
             }
         }
 
+        // weights m = 1..N: odd weights first, then even ones (sc_m a_mp vanishes
+        // unless p and m have the same parity); the near records of the next
+        // weight in this order are prefetched behind the current one
 #pragma unroll 1
-        for (int m = 1; m <= N; ++m) {
-            // coefficient sets of weight m for rows k = 0..N, staged per lane
-            {
-                float cf[NL];
+        for (int it = 0; it < N; ++it) {
+            const int m = it < (N + 1) / 2 ? 2 * it + 1 : 2 * (it - (N + 1) / 2) + 2;
+            if (m & 1) far_sets<N, 1>(m, U, V, s_set, lane);
+            else far_sets<N, 0>(m, U, V, s_set, lane);
+            const float *o = s_set + lane;
+            // row k = 0: velocity panel P0 only
+            if (PANELS) {
+                float X[3], Y[3], Z[3];
+                far_xyz(o, D, t, p, X, Y, Z);
+                const float AI = o[0];
 #pragma unroll
-                for (int pp = 0; pp < NL; ++pp) cf[pp] = c_leg32[m][pp];
-                float R0[N + 3], C0[N + 2], R1[N + 2];
+                for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
-                for (int k = 0; k < N + 3; ++k) {
-                    float s1 = 0.f;
-#pragma unroll
-                    for (int pp = 0; pp < NL; ++pp) s1 = fmaf(cf[pp], V[pp][k], s1);
-                    R0[k] = s1;
-                }
-#pragma unroll
-                for (int k = 0; k < N + 2; ++k) {
-                    float s1 = 0.f;
-#pragma unroll
-                    for (int pp = 0; pp < NL; ++pp) s1 = fmaf(cf[pp], V[pp + 1][k], s1);
-                    C0[k] = -s1;
-                }
-#pragma unroll
-                for (int k = 0; k < N + 2; ++k)
-                    R1[k] = (float)bonnet_a(k) * R0[k + 1] + (k > 0 ? (float)bonnet_b(k) * R0[k > 0 ? k - 1 : 0] : 0.f);
-#pragma unroll
-                for (int k = 0; k < NL; ++k) {
-                    float ai = 0.f, ee = 0.f;
-#pragma unroll
-                    for (int pp = 0; pp < NL; ++pp) {
-                        ai = fmaf(cf[pp], U[pp][k], ai);
-                        ee = fmaf(cf[pp], V[pp + 2][k], ee);
-                    }
-                    float *o = s_set + k * 7 * 32 + lane;
-                    o[0] = ai;
-                    o[32] = R0[k];
-                    o[64] = R1[k];
-                    o[96] = (float)bonnet_a(k) * R1[k + 1] + (k > 0 ? (float)bonnet_b(k) * R1[k > 0 ? k - 1 : 0] : 0.f);
-                    o[128] = C0[k];
-                    o[160] = (float)bonnet_a(k) * C0[k + 1] + (k > 0 ? (float)bonnet_b(k) * C0[k > 0 ? k - 1 : 0] : 0.f);
-                    o[192] = ee;
-                }
+                    for (int aa = 0; aa < 3; ++aa)
+                        s_pan[bb * 96 + lane * 3 + aa] =
+                            sv * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * Y[bb] + p[aa] * Z[bb]);
             }
-#pragma unroll 1
-            for (int k = 0; k <= N; ++k) {
-                const float *o = s_set + k * 7 * 32 + lane;
-                const float AI = o[0], R0 = o[32], R1 = o[64], R2 = o[96], C0 = o[128], C1 = o[160], E = o[192];
+            // row k = 1: block row D1 t (theta t)^T and velocity panel P1
+            {
+                const float *o1 = o + 7 * 32;
                 float X[3], Y[3], Z[3], Q[3];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    X[c] = R0 * D[c] + R1 * t[c] + C0 * p[c];
-                    Y[c] = R1 * D[c] + R2 * t[c] + C1 * p[c];
-                    Z[c] = C0 * D[c] + C1 * t[c] + E * p[c];
-                }
+                far_xyz(o1, D, t, p, X, Y, Z);
+                const float AI = o1[0];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) Q[c] = AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c];
-                if (k >= 1) {
-                    const float g = s_gk[k], ek = s_gk[8 + k];
-                    float *dst = s_stg + lane * RB + 3 * (k - 1);
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa) s_stg[bb * GR + lane * RB + aa] = D1 * t[aa] * Q[bb];
+                if (PANELS) {
 #pragma unroll
                     for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
-                        for (int aa = 0; aa < 3; ++aa) {
-                            float v = (k == 1) ? D1 * t[aa] * Q[bb]
-                                               : g * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] +
-                                                      t[aa] * (Y[bb] - ek * Q[bb]) + p[aa] * Z[bb]);
-                            if (diag) v = (k == m && aa == bb) ? 1.f : 0.f;
-                            dst[bb * GR + aa] = v;
-                        }
+                        for (int aa = 0; aa < 3; ++aa)
+                            s_pan[(3 + bb) * 96 + lane * 3 + aa] =
+                                sw * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * (Y[bb] - Q[bb]) + p[aa] * Z[bb]);
                 }
-                if (PANELS && k <= 1) {
+            }
+            // rows k = 2..N: gamma_k (theta - E_k t (theta t)^T)
+#pragma unroll 1
+            for (int k = 2; k <= N; ++k) {
+                const float *ok = o + k * 7 * 32;
+                float X[3], Y[3], Z[3], W[3];
+                far_xyz(ok, D, t, p, X, Y, Z);
+                const float AI = ok[0], g = s_gk[k], ek = s_gk[8 + k];
 #pragma unroll
-                    for (int bb = 0; bb < 3; ++bb)
+                for (int c = 0; c < 3; ++c) W[c] = Y[c] - ek * (AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c]);
+                float *dst = s_stg + lane * RB + 3 * (k - 1);
 #pragma unroll
-                        for (int aa = 0; aa < 3; ++aa) {
-                            const float th = (aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * Y[bb] + p[aa] * Z[bb];
-                            const float v = (k == 0) ? sv * th : sw * (th - Q[bb] * t[aa]);
-                            s_pan[(k * 3 + bb) * 96 + lane * 3 + aa] = diag ? 0.f : v;
-                        }
-                }
+                for (int bb = 0; bb < 3; ++bb)
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa)
+                        dst[bb * GR + aa] = g * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * W[bb] + p[aa] * Z[bb]);
+            }
+            // the diagonal pair (its projections are zero): identity where k = m
+            if (diag) {
+#pragma unroll
+                for (int aa = 0; aa < 3; ++aa) s_stg[aa * GR + lane * RB + 3 * (m - 1) + aa] = 1.f;
             }
             cp_async_wait_all();
             __syncwarp();
             // near pairs: the FP64-integrated columns of weight m replace the
-            // staged zeros, one (near lane, entry) per thread
-            {
-                constexpr int PER = 3 * RB + (PANELS ? 18 : 0);
-                for (int idx = lane; idx < nnear * PER; idx += 32) {
-                    const int r = idx / PER, e = idx - r * PER;
-                    const int L = s_nl[r];
-                    int dst;
-                    if (e < 3 * RB) {
-                        const int bb = e / RB, rr = e - bb * RB;
-                        dst = bb * GR + L * RB + rr;
-                    } else {
-                        const int e2 = e - 3 * RB, w = e2 / 9, rem = e2 - w * 9, bb = rem / 3, aa = rem - bb * 3;
-                        dst = 3 * GR + (w * 3 + bb) * 96 + L * 3 + aa;  // s_pan follows s_stg
-                    }
-                    s_stg[dst] = s_nb[r * kNearWeight + e];
-                }
+            // staged zeros; entry offsets are fixed per thread
+            for (int r = 0; r < nnear; ++r) {
+                const int L = s_nl[r];
+                const float *src = s_nb + r * kNearWeight;
+                if (lane < 3 * RB) s_stg[moff0 + L * RB] = src[lane];
+                if (lane < 3 * RB - 32) s_stg[moff1 + L * RB] = src[lane + 32];
+                if (PANELS && lane < 18) s_stg[poff + L * 3] = src[3 * RB + lane];
             }
             __syncwarp();
-            // the records of weight m+1, hidden behind the stores and the next weight
-            if (m < N) {
+            // the records of the next weight, hidden behind the stores and that weight's work
+            if (it + 1 < N) {
+                const int mn = it + 1 < (N + 1) / 2 ? 2 * it + 3 : 2 * (it + 1 - (N + 1) / 2) + 2;
                 for (int u = lane; u < nnear * (kNearWeight / 4); u += 32) {
-                    const int r = u / (kNearWeight / 4), c = u - r * (kNearWeight / 4);
+                    const int r = u >> 4, c = u & 15;
                     cp_async16(s_nb + r * kNearWeight + 4 * c,
-                               a.nearbuf + (int64_t)s_ns[r] * kNearBlock + m * kNearWeight + 4 * c);
+                               a.nearbuf + (int64_t)s_ns[r] * kNearBlock + (mn - 1) * kNearWeight + 4 * c);
                 }
                 cp_async_commit();
             }
