@@ -143,12 +143,12 @@ struct PairTensors {
 template <int N>
 __device__ __forceinline__ void moments_near(double b, double c, double *I, double *J, double *S) {
     constexpr int K = N + 3;
-    const double ue = sqrt(1.0 + b + c);
-    const double ub = sqrt(1.0 - b + c);
+    const double xe = 1.0 + b + c, xb = 1.0 - b + c;
+    const double iue = rsqrt(xe), iub = rsqrt(xb);
+    const double ue = xe * iue, ub = xb * iub;
     const double te = 1.0 + 0.5 * b;
     const double tb = -1.0 + 0.5 * b;
     const double d = c - 0.25 * b * b;
-    const double iue = 1.0 / ue, iub = 1.0 / ub;
     I[0] = log(fabs((2.0 + b + 2.0 * ue) / (-2.0 + b + 2.0 * ub)));
     I[1] = ue - ub - 0.5 * b * I[0];
     if (d < 1e-14) {
@@ -722,7 +722,7 @@ struct NearSmem {
     static constexpr int BLK = kNearBlock / 2;          // staged block + panels (floats)
     static constexpr int RHS = 3 * (N + 1) + 1;
     static constexpr int WARP = X + TM + BLK + RHS + ((X + TM + BLK + RHS) & 1);
-    static constexpr int TABLES = 8 * kMaxLQ + kMaxLQ + 72 + 16;   // w P, s, Legendre coefficients, Bonnet
+    static constexpr int TABLES = 8 * kMaxLQ + kMaxLQ + 72 + 32;   // w P, s, Legendre coefficients, row constants
     // every per-warp region and the staged block (read as float4) start on 16 bytes
     static_assert(X % 2 == 0 && (X + TM) % 2 == 0 && WARP % 2 == 0 && TABLES % 2 == 0, "16-byte alignment");
     static size_t bytes() { return sizeof(double) * (TABLES + (size_t)kNearWarps * WARP); }
@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
     double *s_wP = reinterpret_cast<double *>(smem_raw);   // [8][kMaxLQ]
     double *s_pv = s_wP + 8 * kMaxLQ;
     double *s_leg = s_pv + kMaxLQ;                          // [8][9]: sc_m a_mp (odd row stride)
-    double *s_bon = s_leg + 72;                             // alpha_k (0..7), beta_k (8..15)
+    double *s_bon = s_leg + 72;                             // alpha_k, beta_k, gamma_k, E_k (8 each)
     double *base = s_wP + SM::TABLES + (size_t)warp * SM::WARP;
     double *X = base;
     double *Tm = X + SM::X;
@@ -767,6 +767,8 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
     for (int t = threadIdx.x; t < 8; t += blockDim.x) {
         s_bon[t] = bonnet_a(t);
         s_bon[8 + t] = bonnet_b(t);
+        s_bon[16 + t] = t <= N ? tab.gamma[t] : 0.0;
+        s_bon[24 + t] = t <= N ? tab.Ek[t] : 0.0;
     }
     for (int t = lane; t < SM::X; t += 32) X[t] = 0.0;
     for (int t = lane; t < NRHS; t += 32) rhs[t] = 0.0;
@@ -819,10 +821,14 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
             Tm[(lane >> 2) * kTmLd + 8 * tile + 2 * (lane & 3) + 1] = d1;
         }
         __syncwarp();
-        PairTensors<double> P;
-        P.set(D, t, p);
+        const double Dt = D[0] * t[0] + D[1] * t[1] + D[2] * t[2];
+        const double tt = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+        const double pt = p[0] * t[0] + p[1] * t[1] + p[2] * t[2];
+        // one (weight m, row k) per thread: the N*(N+1) pairs with m >= 1 first,
+        // then the N+1 right-hand-side rows of weight 0 (cheaper) in what is left
         for (int u = lane; u < NL * NL; u += 32) {
-            const int m = u / NL, k = u - m * NL;
+            const int m = u < N * NL ? u / NL + 1 : 0;
+            const int k = u < N * NL ? u - (m - 1) * NL : u - N * NL;
             const double *lg = s_leg + m * 9;
             // coefficient sets of weight m at rows k-2..k+2
             double AI = 0.0, E = 0.0, R0[5] = {0, 0, 0, 0, 0}, C0[3] = {0, 0, 0};
@@ -847,37 +853,52 @@ __global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a
             const double R1 = al[k] * R0[3] + be[k] * R0[1];
             const double R2 = al[k] * R1p + be[k] * R1m;
             const double C1 = al[k] * C0[2] + be[k] * C0[0];
-            double th[6];
+            // theta = AI I + D X^T + t Y^T + p Z^T,  Q = theta t
+            double X[3], Y[3], Z[3], Q[3];
 #pragma unroll
-            for (int c = 0; c < 6; ++c)
-                th[c] = (c < 3 ? AI : 0.0) + R0[2] * P.DD[c] + R1 * P.DT[c] + R2 * P.TT[c] + C0[1] * P.PD[c] +
-                        C1 * P.PT[c] + E * P.PP[c];
+            for (int c = 0; c < 3; ++c) {
+                X[c] = R0[2] * D[c] + R1 * t[c] + C0[1] * p[c];
+                Y[c] = R1 * D[c] + R2 * t[c] + C1 * p[c];
+                Z[c] = C0[1] * D[c] + C1 * t[c] + E * p[c];
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) Q[c] = AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c];
             if (m == 0) {
-                rhs[3 * k + 0] += th[0] * f[0] + th[3] * f[1] + th[4] * f[2];
-                rhs[3 * k + 1] += th[3] * f[0] + th[1] * f[1] + th[5] * f[2];
-                rhs[3 * k + 2] += th[4] * f[0] + th[5] * f[1] + th[2] * f[2];
+                const double Xf = X[0] * f[0] + X[1] * f[1] + X[2] * f[2];
+                const double Yf = Y[0] * f[0] + Y[1] * f[1] + Y[2] * f[2];
+                const double Zf = Z[0] * f[0] + Z[1] * f[1] + Z[2] * f[2];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) rhs[3 * k + c] += AI * f[c] + D[c] * Xf + t[c] * Yf + p[c] * Zf;
                 continue;
             }
-            double Q[3];
-#pragma unroll
-            for (int bb = 0; bb < 3; ++bb)
-                Q[bb] = th[sym_index(bb, 0)] * t[0] + th[sym_index(bb, 1)] * t[1] + th[sym_index(bb, 2)] * t[2];
+            float *rec = blk + (m - 1) * kNearWeight;
             if (k >= 1) {
-                const double gk = tab.gamma[k], ek = tab.Ek[k];
+                // k = 1: D1 t Q^T; k >= 2: gamma_k (theta - E_k t Q^T); one formula
+                // g (AI' I + D X'^T + t W^T + p Z'^T) with the row's coefficients
+                const bool one = k == 1;
+                const double g = one ? D1 : s_bon[16 + k], ek = s_bon[24 + k];
+                const double ai = one ? 0.0 : AI;
+                double W[3];
 #pragma unroll
-                for (int bb = 0; bb < 3; ++bb)
+                for (int c = 0; c < 3; ++c) W[c] = one ? Q[c] : Y[c] - ek * Q[c];
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) {
+                    const double xb = one ? 0.0 : X[bb], zb = one ? 0.0 : Z[bb];
 #pragma unroll
                     for (int aa = 0; aa < 3; ++aa)
-                        blk[(m - 1) * kNearWeight + bb * RB + 3 * (k - 1) + aa] =
-                            (float)((k == 1) ? D1 * t[aa] * Q[bb] : gk * (th[sym_index(aa, bb)] - ek * t[aa] * Q[bb]));
+                        rec[bb * RB + 3 * (k - 1) + aa] =
+                            (float)(g * ((aa == bb ? ai : 0.0) + D[aa] * xb + t[aa] * W[bb] + p[aa] * zb));
+                }
             }
             if (PANELS && k <= 1) {
+                // P0: sv theta; P1: sw (theta - t Q^T)
+                const double sc = k == 0 ? sv : sw, kq = k == 0 ? 0.0 : 1.0;
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
                     for (int aa = 0; aa < 3; ++aa)
-                        blk[(m - 1) * kNearWeight + 3 * RB + k * 9 + bb * 3 + aa] = (float)(
-                            (k == 0) ? sv * th[sym_index(aa, bb)] : sw * (th[sym_index(aa, bb)] - Q[bb] * t[aa]));
+                        rec[3 * RB + k * 9 + bb * 3 + aa] = (float)(
+                            sc * ((aa == bb ? AI : 0.0) + D[aa] * X[bb] + t[aa] * (Y[bb] - kq * Q[bb]) + p[aa] * Z[bb]));
             }
         }
         __syncwarp();
