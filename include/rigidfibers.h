@@ -98,7 +98,9 @@ typedef struct rf_params {
     int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 12) */
     double inner_tol;                    /* mixed precision: inner GMRES relative tolerance (default 3e-3) */
     double near_field_c;                 /* mixed precision: squared distance below which the analytic
-                                            integral stays FP64 (default 10, the recursion switch);
+                                            integral stays FP64 (default 6: from there on the FP32
+                                            backward recursion reaches FP32 accuracy; raised to 10
+                                            where the tile kernel runs: numeric integration, N > 5);
                                             >= 1e30 keeps every integral in FP64 */
     int32_t reserved[8];
 } rf_params;

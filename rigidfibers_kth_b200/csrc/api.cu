@@ -217,7 +217,7 @@ void rf_params_default(rf_params *p) {
     p->max_refinements = 30;
     p->cluster_size = 12;
     p->inner_tol = 3e-3;
-    p->near_field_c = 10.0;
+    p->near_field_c = 6.0;
 }
 
 const char *rf_status_string(rf_status s) {
@@ -472,7 +472,12 @@ rf_status rf_assemble_system(rf_handle *h) {
         a.near_c = 0.0;        // plain FP32 method: every pair in FP32
         a.axis_ratio = 0.0;
     } else {
-        a.near_c = h->p.near_field_c > 0.0 ? h->p.near_field_c : 10.0;
+        // FP64 below near_c: at least rf::kSplitMinNearC for the split kernels
+        // (their FP32 far field runs the backward recursion, accurate there),
+        // at least 10 for the tile kernel (whose FP32 points below 10 would run
+        // the forward recursion)
+        const double want = h->p.near_field_c > 0.0 ? h->p.near_field_c : rf::kSplitMinNearC;
+        a.near_c = std::max(want, h->split ? rf::kSplitMinNearC : 10.0);
         a.axis_ratio = 1.0 / 16.0;
     }
     if (h->split) {
@@ -511,16 +516,31 @@ rf_status rf_assemble_system(rf_handle *h) {
             CK(h, cudaStreamSynchronize(h->stream), "near-pair count");
             h->near_pairs = *hcount;
             if (h->near_pairs > h->near_cap) {
+                // a reallocation of gigabytes costs hundreds of milliseconds and a
+                // settling suspension keeps gaining near pairs, so grow to the
+                // largest of twice the count, a quarter of all pairs and a quarter
+                // of the free device memory (at most all pairs); on failure try
+                // the count itself
                 cudaFree(h->nearbuf);
                 h->nearbuf = nullptr;
                 h->near_cap = 0;
-                const int64_t cap = std::min<int64_t>((int64_t)h->M * (h->M - 1), h->near_pairs + h->near_pairs / 4 + 1024);
-                if (cudaMalloc(&h->nearbuf, sizeof(float) * rf::kNearBlockFloats * (size_t)cap) == cudaSuccess) {
-                    h->near_cap = cap;
-                } else {
-                    (void)cudaGetLastError();  // out of memory: write the near blocks into A directly
+                const int64_t all = (int64_t)h->M * (h->M - 1);
+                const int64_t rec = (int64_t)sizeof(float) * rf::kNearBlockFloats;
+                size_t free_b = 0, total_b = 0;
+                if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+                    (void)cudaGetLastError();
+                    free_b = 0;
+                }
+                const int64_t want = std::max<int64_t>({2 * h->near_pairs + 1024, all / 4, (int64_t)(free_b / 4) / rec});
+                for (int64_t cap : {std::min<int64_t>(all, want), std::min<int64_t>(all, h->near_pairs)}) {
+                    if (cudaMalloc(&h->nearbuf, sizeof(float) * rf::kNearBlockFloats * (size_t)cap) == cudaSuccess) {
+                        h->near_cap = cap;
+                        break;
+                    }
+                    (void)cudaGetLastError();  // out of memory
                     h->nearbuf = nullptr;
                 }
+                // still none: the near kernel writes its blocks into A directly
             }
             direct = h->near_pairs > h->near_cap;
             sa.nearbuf = h->nearbuf;

@@ -5,10 +5,10 @@
 //
 // The mixed path stores A in FP32 (and BF16).  A fiber pair (i, j) is "near"
 // when one of target i's quadrature points lies within sqrt(near_c) of source
-// j's centre or close to its axis beyond its ends (the forward-recursion range
-// of the reference, c < 10, and the cancellation-prone closed forms).  Near
-// pairs (about a sixth of the pairs in a dense cloud) are integrated in FP64,
-// far pairs in FP32.  Three kernels:
+// j's centre (default c < 6: closer, the FP32 backward recursion from n = 27
+// loses digits; the reference itself switches to forward recursion below 10)
+// or close to its axis beyond its ends (cancellation-prone closed forms).
+// Near pairs are integrated in FP64, far pairs in FP32.  Three kernels:
 //   classify_kernel   one warp per target: near-pair bitmap and per-target
 //                     lists in ascending source order;
 //   far_pairs_kernel  FP32, lane = target fiber, warp-uniform source: every
@@ -712,6 +712,9 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
 
 // ---------------------------------------------------------------- near pairs (FP64)
 constexpr int kNearWarps = 4;
+#ifndef RF_NEAR_MINB
+#define RF_NEAR_MINB 4
+#endif
 constexpr int kXq = 52;  // q stride of X[col][q]: 52 = 4 mod 16 makes the B fragments conflict-free
 constexpr int kTmLd = 17;  // row stride of the projections Tm[k][col] (odd: rows fall in different banks)
 
@@ -735,7 +738,7 @@ struct NearSmem {
 // its column stores) or straight into A (DIRECT = true, used when the buffer
 // could not be grown).
 template <int N, bool PANELS, bool DIRECT>
-__global__ void __launch_bounds__(kNearWarps * 32) near_pairs_kernel(SplitArgs a) {
+__global__ void __launch_bounds__(kNearWarps * 32, RF_NEAR_MINB) near_pairs_kernel(SplitArgs a) {
     using SD = SplitDims<N>;
     using SM = NearSmem<N>;
     constexpr int NL = SD::NL, NV = SD::NV, RB = SD::RB, NRHS = SD::NRHS;
@@ -1003,10 +1006,10 @@ cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st) {
 
 cudaError_t launch_split_far(const SplitArgs &a, int far_chunks, cudaStream_t st) {
     const bool panels = a.PV32 != nullptr;
-    // far pairs have c >= near_c and d >= c * axis_ratio: with the defaults
-    // (near_c >= 10, axis_ratio >= 1e-6) only the backward recursion and the
-    // regular closed forms can occur
-    const bool far_only = a.near_bits != nullptr && a.near_c >= 10.0 && a.axis_ratio >= 1e-6;
+    // far pairs have c >= near_c >= kSplitMinNearC and d >= c * axis_ratio:
+    // the backward recursion (accurate in FP32 there) and the regular closed
+    // forms cover every point
+    const bool far_only = a.near_bits != nullptr && a.near_c >= kSplitMinNearC && a.axis_ratio >= 1e-6;
     switch (a.N) {
 #define RF_FAR_CASE(n)                                                                                     \
     case n:                                                                                                \

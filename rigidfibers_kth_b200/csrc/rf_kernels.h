@@ -63,6 +63,10 @@ struct SplitArgs {
     double axis_ratio;         // d < c*axis_ratio makes a pair near
 };
 constexpr int kNearBlockFloats = 320;
+// Smallest near threshold of the split assembly: from c = 6 on, the FP32
+// backward recursion from n = 27 is accurate to FP32 rounding at n <= N+2 (its
+// truncation error falls like c^(-(27-n)/2), 6^-10 = 1.7e-8).
+constexpr double kSplitMinNearC = 6.0;
 bool split_supported(int N, int LQ);
 int split_far_chunks(int M, int sm_count);
 cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st);

@@ -44,7 +44,7 @@ class FiberParams:
     max_refinements: int = 30
     cluster_size: int = 12
     inner_tol: float = 3e-3
-    near_field_c: float = 10.0
+    near_field_c: float = 6.0
 
     def to_c(self):
         p = L.RfParams()
