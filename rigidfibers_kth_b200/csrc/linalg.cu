@@ -23,36 +23,42 @@ namespace rf {
 
 namespace {
 
+// 16 bytes of A per thread and column: raw() issues the streaming load,
+// get() converts the raw bits to the accumulation type.  The GEMV issues all
+// loads of an unrolled column group before converting any, so that every
+// load is in flight at once.
 template <typename S>
 struct Vec16;
 template <>
 struct Vec16<double> {
     static constexpr int kVec = 2;
+    __device__ __forceinline__ static uint4 raw(const double *p) { return __ldcs(reinterpret_cast<const uint4 *>(p)); }
     template <typename ACC>
-    __device__ __forceinline__ static void load(const double *p, ACC *v) {
-        const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
-        v[0] = (ACC)t.x;
-        v[1] = (ACC)t.y;
+    __device__ __forceinline__ static void get(const uint4 &t, ACC *v) {
+        v[0] = (ACC)__hiloint2double((int)t.y, (int)t.x);
+        v[1] = (ACC)__hiloint2double((int)t.w, (int)t.z);
     }
 };
 template <>
 struct Vec16<float> {
     static constexpr int kVec = 4;
+    __device__ __forceinline__ static uint4 raw(const float *p) { return __ldcs(reinterpret_cast<const uint4 *>(p)); }
     template <typename ACC>
-    __device__ __forceinline__ static void load(const float *p, ACC *v) {
-        const float4 t = __ldcs(reinterpret_cast<const float4 *>(p));
-        v[0] = (ACC)t.x;
-        v[1] = (ACC)t.y;
-        v[2] = (ACC)t.z;
-        v[3] = (ACC)t.w;
+    __device__ __forceinline__ static void get(const uint4 &t, ACC *v) {
+        v[0] = (ACC)__uint_as_float(t.x);
+        v[1] = (ACC)__uint_as_float(t.y);
+        v[2] = (ACC)__uint_as_float(t.z);
+        v[3] = (ACC)__uint_as_float(t.w);
     }
 };
 template <>
 struct Vec16<__nv_bfloat16> {
     static constexpr int kVec = 8;
+    __device__ __forceinline__ static uint4 raw(const __nv_bfloat16 *p) {
+        return __ldcs(reinterpret_cast<const uint4 *>(p));
+    }
     template <typename ACC>
-    __device__ __forceinline__ static void load(const __nv_bfloat16 *p, ACC *v) {
-        const uint4 t = __ldcs(reinterpret_cast<const uint4 *>(p));
+    __device__ __forceinline__ static void get(const uint4 &t, ACC *v) {
         const uint32_t w[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -82,22 +88,24 @@ __global__ void __launch_bounds__(kGemvThreads) gemv_partial_kernel(const S *__r
         const S *p = A + c0 * lda + row;
         int64_t c = c0;
         for (; c + kGemvUnroll <= c1; c += kGemvUnroll) {
-            ACC a[kGemvUnroll][VEC];
+            uint4 raw[kGemvUnroll];
             ACC xv[kGemvUnroll];
 #pragma unroll
+            for (int u = 0; u < kGemvUnroll; ++u) raw[u] = Vec16<S>::raw(p + (int64_t)u * lda);
+#pragma unroll
+            for (int u = 0; u < kGemvUnroll; ++u) xv[u] = (ACC)__ldg(x + c + u);
+#pragma unroll
             for (int u = 0; u < kGemvUnroll; ++u) {
-                Vec16<S>::load(p + (int64_t)u * lda, a[u]);
-                xv[u] = (ACC)__ldg(x + c + u);
+                ACC a[VEC];
+                Vec16<S>::get(raw[u], a);
+#pragma unroll
+                for (int v = 0; v < VEC; ++v) acc[v] += a[v] * xv[u];
             }
-#pragma unroll
-            for (int u = 0; u < kGemvUnroll; ++u)
-#pragma unroll
-                for (int v = 0; v < VEC; ++v) acc[v] += a[u][v] * xv[u];
             p += (int64_t)kGemvUnroll * lda;
         }
         for (; c < c1; ++c) {
             ACC a[VEC];
-            Vec16<S>::load(p, a);
+            Vec16<S>::get(Vec16<S>::raw(p), a);
             const ACC xv = (ACC)__ldg(x + c);
 #pragma unroll
             for (int v = 0; v < VEC; ++v) acc[v] += a[v] * xv;
@@ -136,12 +144,15 @@ int gemv_slots(int sm_count) {
     return sm_count * occ;
 }
 
-// Column splits: about kWaves full waves of resident CTAs, so that the last,
-// partial wave costs little; at least 64 columns per split.
-constexpr int kWaves = 8;
+// Column splits: a few full waves of resident CTAs, so that the last, partial
+// wave costs little; at least 64 columns per split.
+// BF16 (8 elements per load) prefers 4 waves: its many row-tile-narrow splits
+// otherwise write and re-read ~80 MB of partial sums per product at M = 4000
+// (measured 1.029 vs 1.096 ms; FP32 and FP64 are best at 8).
 int gemv_splits(int64_t m, int64_t k, int vec, int slots) {
+    const int waves = vec >= 8 ? 4 : 8;
     const int64_t tiles = (m + (int64_t)kGemvThreads * vec - 1) / ((int64_t)kGemvThreads * vec);
-    int64_t splits = ((int64_t)kWaves * slots + tiles - 1) / tiles;
+    int64_t splits = ((int64_t)waves * slots + tiles - 1) / tiles;
     const int64_t max_by_cols = k / 64 > 0 ? k / 64 : 1;
     if (splits > max_by_cols) splits = max_by_cols;
     if (splits < 1) splits = 1;
