@@ -47,7 +47,7 @@ L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes (read + write) per stored element of A of one BF16 product, from
 # the ncu capture summarised in profiles/gemv_bf16_m1000.md; scaled to the
 # workload's matrix size (the traffic grows with the elements streamed)
-TRAFFIC_PER_ELEMENT = (451.270400e6 + 7.941632e6) / (15040 * 15000)
+TRAFFIC_PER_ELEMENT = (451.270656e6 + 7.171840e6) / (15040 * 15000)
 
 
 def parse_args():
