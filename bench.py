@@ -66,16 +66,23 @@ def parse_args():
 
 
 # ---------------------------------------------------------------- distributed
-def dist_setup():
+def dist_setup(timeout_s=300):
+    """One process per GPU (torchrun env); NCCL with GPUs, gloo without (CPU tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
+        import datetime
+
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            backend = "nccl"
+        else:
+            backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return world, rank, local
 
 
@@ -92,7 +99,8 @@ def max_over_ranks(v, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -470,7 +470,6 @@ rf_status rf_assemble_system(rf_handle *h) {
     const int prec = h->p.precision;
     if (prec == RF_PREC_FP32) {
         a.near_c = 0.0;        // plain FP32 method: every pair in FP32
-        a.axis_ratio = 0.0;
     } else {
         // FP64 below near_c: at least rf::kSplitMinNearC for the split kernels
         // (their FP32 far field runs the backward recursion, accurate there),
@@ -478,7 +477,6 @@ rf_status rf_assemble_system(rf_handle *h) {
         // the forward recursion)
         const double want = h->p.near_field_c > 0.0 ? h->p.near_field_c : rf::kSplitMinNearC;
         a.near_c = std::max(want, h->split ? rf::kSplitMinNearC : 10.0);
-        a.axis_ratio = 1.0 / 16.0;
     }
     if (h->split) {
         rf::SplitArgs sa{};
@@ -505,7 +503,6 @@ rf_status rf_assemble_system(rf_handle *h) {
         sa.near_contr = h->near_contr;
         sa.chunk = h->far_chunk;
         sa.near_c = a.near_c;
-        sa.axis_ratio = a.axis_ratio;
         bool direct = false;
         if (h->near_bits) {
             CK(h, rf::launch_split_classify(sa, h->stream), "near-pair classification");

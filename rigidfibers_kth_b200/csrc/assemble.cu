@@ -148,8 +148,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
             }
         } else {
             // Mixed precision in two passes: FP32 for the far field, then the
-            // points near the source fiber (c < near_c) or close to its axis
-            // beyond the ends (d < c * axis_ratio) in FP64, compacted onto
+            // points near the source fiber (c < near_c) in FP64, compacted onto
             // consecutive threads so that no warp carries both paths.
             if (tid == 0) s_nlist = 0;
             __syncthreads();
@@ -158,10 +157,8 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
                 bool need64 = false;
                 if (i < a.M && i != j) {
                     const double r0x = xbx - xs0, r0y = xby - xs1, r0z = xbz - xs2;
-                    const double bq = -2.0 * (ts0 * r0x + ts1 * r0y + ts2 * r0z);
                     const double cq = r0x * r0x + r0y * r0y + r0z * r0z;
-                    const double dq = cq - 0.25 * bq * bq;
-                    need64 = NUMERIC ? (cq < a.near_c) : (cq < a.near_c || dq < cq * a.axis_ratio);
+                    need64 = cq < a.near_c;
                     if (!need64) {
                         if (NUMERIC) {
                             float G[NL][6];

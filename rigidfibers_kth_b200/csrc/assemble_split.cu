@@ -5,10 +5,12 @@
 //
 // The mixed path stores A in FP32 (and BF16).  A fiber pair (i, j) is "near"
 // when one of target i's quadrature points lies within sqrt(near_c) of source
-// j's centre (default c < 6: closer, the FP32 backward recursion from n = 27
-// loses digits; the reference itself switches to forward recursion below 10)
-// or close to its axis beyond its ends (cancellation-prone closed forms).
-// Near pairs are integrated in FP64, far pairs in FP32.  Three kernels:
+// j's centre (default c < 6: closer, the FP32 backward recursion loses digits;
+// the reference itself switches to forward recursion below 10).  Near pairs
+// are integrated in FP64, far pairs in FP32, every moment of a far pair by the
+// backward recursion run down to n = 0 (moments_backward_fp32: none of the
+// reference's n = 0, 1 closed forms, which cancel for distant pairs and close
+// to the source axis).  Three kernels:
 //   classify_kernel   one warp per target: near-pair bitmap and per-target
 //                     lists in ascending source order;
 //   far_pairs_kernel  FP32, lane = target fiber, warp-uniform source: every
@@ -227,14 +229,11 @@ __global__ void __launch_bounds__(kClassifyWarps * 32) classify_kernel(SplitArgs
         bool near = false;
         if (j < a.M && j != i) {
             const double D0 = xi0 - a.pos[3 * j], D1 = xi1 - a.pos[3 * j + 1], D2 = xi2 - a.pos[3 * j + 2];
-            const double p0 = a.ori[3 * j], p1 = a.ori[3 * j + 1], p2 = a.ori[3 * j + 2];
             for (int q = 0; q < a.LQ && !near; ++q) {
                 const double s = s_pv[q];
                 const double r0 = D0 + s * ti0, r1 = D1 + s * ti1, r2 = D2 + s * ti2;
                 const double c = r0 * r0 + r1 * r1 + r2 * r2;
-                const double b = -2.0 * (p0 * r0 + p1 * r1 + p2 * r2);
-                const double d = c - 0.25 * b * b;
-                near = (c < a.near_c) || (d < c * a.axis_ratio);
+                near = c < a.near_c;
             }
         }
         const unsigned mask = __ballot_sync(0xffffffffu, near);
@@ -398,47 +397,6 @@ __device__ __forceinline__ void far_xyz(const float *o, const float *D, const fl
     }
 }
 
-// FP32 moments of a far pair (c >= 10, d >= c/16 at every point): the regular
-// closed forms without cancellation (te/ue - tb/ub rewritten when te and tb
-// share a sign, the logarithm argument formed stably), the hardware reciprocal
-// square root and reciprocal, and the backward recursion from n = 27 with the
-// per-item factors 1/c, b/c, (ue -+ ub)/c taken out of the loop.
-template <int N>
-__device__ __forceinline__ void far_moments(float b, float c, float *I, float *J, float *S) {
-    constexpr int K = N + 3;
-    const float xe = 1.0f + b + c, xb = 1.0f - b + c;
-    const float iue = rsqrtf(xe), iub = rsqrtf(xb);
-    const float ue = xe * iue, ub = xb * iub;
-    const float te = 1.0f + 0.5f * b, tb = -1.0f + 0.5f * b;
-    const float d = c - 0.25f * b * b;
-    const float id = __fdividef(1.0f, d);
-    const float ae = (te >= 0.f) ? (te + ue) : __fdividef(d, ue - te);
-    const float ab = (tb >= 0.f) ? (tb + ub) : __fdividef(d, ub - tb);
-    I[0] = logf(__fdividef(ae, ab));
-    I[1] = ue - ub - 0.5f * b * I[0];
-    J[0] = (te * tb > 0.f) ? __fdividef(2.0f * b, (te * ub + tb * ue) * ue * ub) : (te * iue - tb * iub) * id;
-    J[1] = -iue + iub - 0.5f * b * J[0];
-    const float iue3 = iue * iue * iue, iub3 = iub * iub * iub;
-    S[0] = ((2.0f + b) * iue3 - (-2.0f + b) * iub3) * (id * (1.0f / 6.0f)) + (2.0f / 3.0f) * id * J[0];
-    S[1] = (-(b + 2.0f * c) * iue3 + (-b + 2.0f * c) * iub3) * (id * (1.0f / 6.0f)) - b * (1.0f / 3.0f) * id * J[0];
-    const float ic = __fdividef(1.0f, c);
-    const float icb = ic * b, icwp = ic * (ue - ub), icwm = ic * (ue + ub);
-    float i1 = 0.f, i2 = 0.f, j1 = 0.f, j2 = 0.f, s1 = 0.f, s2 = 0.f;
-#pragma unroll
-    for (int n = 27; n >= 2; --n) {
-        // I_n = a0/c (r2 (ue - sbp ub) + cb b I_{n+1} - I_{n+2})  (Int_analytical.f90:137-157)
-        const float a0 = (n + 2.0f) / (n + 1.0f);
-        const float r2 = 1.0f / (n + 2.0f);
-        const float cb = (1.0f - 2.0f * (n + 2.0f)) / (2.0f * (n + 2.0f));
-        const float icw = ((n + 1) % 2 == 0) ? icwp : icwm;
-        const float in = fmaf((a0 * cb) * icb, i1, fmaf(-a0 * ic, i2, (a0 * r2) * icw));
-        const float jn = fmaf(ic, in, fmaf(-icb, j1, -ic * j2));
-        const float sn = fmaf(ic, jn, fmaf(-icb, s1, -ic * s2));
-        if (n < K) { I[n] = in; J[n] = jn; S[n] = sn; }
-        i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
-    }
-}
-
 template <int N, bool PANELS, bool FAR>
 __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a) {
     using SD = SplitDims<N>;
@@ -555,8 +513,7 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
                 const float b = -2.0f * (p[0] * r0x + p[1] * r0y + p[2] * r0z);
                 const float c = r0x * r0x + r0y * r0y + r0z * r0z;
                 float I[KW], J[KW], S[KW];
-                if (FAR) far_moments<N>(b, c, I, J, S);
-                else moments_fp32<N, false>(b, c, I, J, S);
+                moments_fp32<N, FAR>(b, c, I, J, S);
                 const float *w = s_w + q * KW;
                 float wk[KW];
 #pragma unroll
@@ -1006,10 +963,9 @@ cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st) {
 
 cudaError_t launch_split_far(const SplitArgs &a, int far_chunks, cudaStream_t st) {
     const bool panels = a.PV32 != nullptr;
-    // far pairs have c >= near_c >= kSplitMinNearC and d >= c * axis_ratio:
-    // the backward recursion (accurate in FP32 there) and the regular closed
-    // forms cover every point
-    const bool far_only = a.near_bits != nullptr && a.near_c >= kSplitMinNearC && a.axis_ratio >= 1e-6;
+    // far pairs have c >= near_c >= kSplitMinNearC at every point: the FP32
+    // backward recursion alone covers them
+    const bool far_only = a.near_bits != nullptr && a.near_c >= kSplitMinNearC;
     switch (a.N) {
 #define RF_FAR_CASE(n)                                                                                     \
     case n:                                                                                                \

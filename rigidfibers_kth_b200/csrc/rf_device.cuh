@@ -132,16 +132,67 @@ __device__ __forceinline__ void moments_fp64(double b, double c, double *I, doub
     }
 }
 
-// FP32 moments for the far field (c >= near_c) of the mixed-precision path.
-// Same recursions; the n = 0, 1 closed forms are rewritten without the
-// cancellation te/ue - tb/ub (which loses all FP32 digits when the target
-// point lies near the source axis): te/ue - tb/ub = 2b d / ((te ub + tb ue) ue ub)
-// when te and tb share a sign.  Callers route points with d < c/16 to FP64.
-// FAR = true: the caller guarantees c >= 10 and d >= 1e-6 c (far pairs of the
-// split assembly), so only the regular closed forms and the backward recursion
-// are compiled.
+// First index of the FP32 backward recursion.  Its starting values
+// I = J = S = 0 at n + 1, n + 2 are wrong by the true moments there; the error
+// reaches n = 0 damped by c^(-n/2) (the recursion's homogeneous solutions grow
+// like |lambda|^n, lambda^2 + b lambda + c = 0, |lambda| = sqrt(c) since
+// d >= 0) times a polynomial in n that is largest for the S moments of a point
+// on the source axis.  From n = 32 that error is below FP32 rounding for every
+// c >= 6 and every direction: with sampled b, the Legendre combinations of the
+// moments stay within 8e-7 of |X_0| (X = I, J, S) at c = 6, 6.5, 7, 8 on and
+// off the axis; from the reference's n = 27 the on-axis S error is 1e-5 at c = 6.
+constexpr int kBackTop = 32;
+
+// FP32 moments by the backward recursion alone, run down to n = 0.  The
+// three-term relations that the reference uses for n >= 2
+// (Int_analytical.f90:137-157, 177-183, 201-206) hold at n = 0 and 1 as well:
+// d/ds[s^(n+1) R] = ((n+2) s^(n+2) + (n+3/2) b s^(n+1) + (n+1) c s^n) / R and
+// s^n / R = s^n (s^2 + b s + c) / R^3.  The reference's n = 0, 1 closed forms
+// (a logarithm of a ratio close to 1, ue - ub - b I_0 / 2, 1/ub - 1/ue and the
+// S_0, S_1 differences over d) cancel by a factor that grows like c: a pair
+// 100 fiber half-lengths apart loses every FP32 digit in them, and at a point
+// near the source axis the 1/d forms cancel too.  The recursion has neither
+// cancellation: ue - ub enters only as 2b / (ue + ub), and d not at all.
+// Accurate for c >= 6 in every direction (see kBackTop).
+template <int N>
+__device__ __forceinline__ void moments_backward_fp32(float b, float c, float *I, float *J, float *S) {
+    constexpr int K = N + 3;
+    const float xe = 1.0f + b + c, xb = 1.0f - b + c;
+    const float ue = xe * rsqrtf(xe), ub = xb * rsqrtf(xb);
+    const float ic = __fdividef(1.0f, c);
+    const float icb = ic * b;
+    const float icwp = __fdividef(2.0f * b, ue + ub) * ic;  // (ue - ub) / c
+    const float icwm = (ue + ub) * ic;
+    float i1 = 0.f, i2 = 0.f, j1 = 0.f, j2 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
+    for (int n = kBackTop; n >= 0; --n) {
+        // I_n = (ue - (-1)^(n+1) ub - (n+3/2) b I_{n+1} - (n+2) I_{n+2}) / ((n+1) c)
+        const float a0 = (n + 2.0f) / (n + 1.0f);
+        const float r2 = 1.0f / (n + 2.0f);
+        const float cb = (1.0f - 2.0f * (n + 2.0f)) / (2.0f * (n + 2.0f));
+        const float icw = ((n + 1) % 2 == 0) ? icwp : icwm;
+        const float in = fmaf((a0 * cb) * icb, i1, fmaf(-a0 * ic, i2, (a0 * r2) * icw));
+        const float jn = fmaf(ic, in, fmaf(-icb, j1, -ic * j2));
+        const float sn = fmaf(ic, jn, fmaf(-icb, s1, -ic * s2));
+        if (n < K) { I[n] = in; J[n] = jn; S[n] = sn; }
+        i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
+    }
+}
+
+// FP32 moments for every point of the plain FP32 method and for the far field
+// (c >= near_c >= 10) of the tile mixed-precision kernel.  For c >= 10 the
+// backward recursion alone (moments_backward_fp32).  Below 10 (plain FP32
+// method only) the reference's closed forms and forward recursion, the closed
+// forms rewritten without the cancellation te/ue - tb/ub (which loses all FP32
+// digits when the target point lies near the source axis):
+// te/ue - tb/ub = 2b d / ((te ub + tb ue) ue ub) when te and tb share a sign.
+// FAR = true: the caller guarantees c >= 6 (far pairs of the split assembly).
 template <int N, bool FAR = false>
 __device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *J, float *S) {
+    if (FAR || c >= 10.0f) {
+        moments_backward_fp32<N>(b, c, I, J, S);
+        return;
+    }
     constexpr int K = N + 3;
     const float ue = sqrtf(1.0f + b + c);
     const float ub = sqrtf(1.0f - b + c);
@@ -154,7 +205,7 @@ __device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *
     const float ab = (tb >= 0.f) ? (tb + ub) : d * __frcp_rn(ub - tb);
     I[0] = logf(ae * __frcp_rn(ab));
     I[1] = ue - ub - 0.5f * b * I[0];
-    if (!FAR && d < 1e-6f * c) {
+    if (d < 1e-6f * c) {
         // point on the source axis: the d -> 0 limits (Int_analytical.f90:162-164, 189-191)
         J[0] = 0.5f * (__frcp_rn(tb * tb) - __frcp_rn(te * te));
         J[1] = -iue + iub - 0.5f * b * J[0];
@@ -173,32 +224,14 @@ __device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *
         S[1] = (-(b + 2.0f * c) * iue3 + (-b + 2.0f * c) * iub3) * (id * (1.0f / 6.0f)) -
                b * (1.0f / 3.0f) * id * J[0];
     }
-    if (!FAR && c < 10.0f) {
 #pragma unroll
-        for (int n = 2; n < K; ++n) {
-            const float nn = n + 1.0f;
-            const float r = 1.0f / (1.0f - nn);
-            const float sbp = (n % 2 == 1) ? 1.0f : -1.0f;
-            I[n] = -ue * r + sbp * ub * r - (0.5f - (nn - 1.0f)) * b * r * I[n - 1] + (nn - 2.0f) * c * r * I[n - 2];
-            J[n] = I[n - 2] - b * J[n - 1] - c * J[n - 2];
-            S[n] = J[n - 2] - b * S[n - 1] - c * S[n - 2];
-        }
-    } else {
-        const float ic = __frcp_rn(c);
-        float i1 = 0.f, i2 = 0.f, j1 = 0.f, j2 = 0.f, s1 = 0.f, s2 = 0.f;
-#pragma unroll
-        for (int n = 27; n >= 2; --n) {
-            const float nn = (float)n;
-            const float a0 = (nn + 2.0f) / (nn + 1.0f);
-            const float r2 = 1.0f / (nn + 2.0f);
-            const float cb = (1.0f - 2.0f * (nn + 2.0f)) / (2.0f * (nn + 2.0f));
-            const float sbp = ((n + 1) % 2 == 0) ? 1.0f : -1.0f;
-            const float in = a0 * ic * (ue * r2 - sbp * ub * r2 + cb * b * i1 - i2);
-            const float jn = ic * (in - b * j1 - j2);
-            const float sn = ic * (jn - b * s1 - s2);
-            if (n < K) { I[n] = in; J[n] = jn; S[n] = sn; }
-            i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
-        }
+    for (int n = 2; n < K; ++n) {
+        const float nn = n + 1.0f;
+        const float r = 1.0f / (1.0f - nn);
+        const float sbp = (n % 2 == 1) ? 1.0f : -1.0f;
+        I[n] = -ue * r + sbp * ub * r - (0.5f - (nn - 1.0f)) * b * r * I[n - 1] + (nn - 2.0f) * c * r * I[n - 2];
+        J[n] = I[n - 2] - b * J[n - 1] - c * J[n - 2];
+        S[n] = J[n - 2] - b * S[n - 1] - c * S[n - 2];
     }
 }
 

@@ -31,7 +31,6 @@ struct AsmArgs {
     double *vpart;             // [nchunks][6M] l = 0 velocity terms (or null)
     int chunk;                 // sources per CTA
     double near_c;             // mixed: c below which the integral stays FP64
-    double axis_ratio;         // mixed: d < c*axis_ratio stays FP64
 };
 
 cudaError_t launch_assemble(const AsmArgs &a, bool numeric, int pmode, int nchunks, cudaStream_t st);
@@ -60,12 +59,11 @@ struct SplitArgs {
     double *near_contr;        // [M][3(N+1)] or null
     int chunk;                 // sources per far-pair CTA
     double near_c;             // c below which a pair is near
-    double axis_ratio;         // d < c*axis_ratio makes a pair near
 };
 constexpr int kNearBlockFloats = 320;
 // Smallest near threshold of the split assembly: from c = 6 on, the FP32
-// backward recursion from n = 27 is accurate to FP32 rounding at n <= N+2 (its
-// truncation error falls like c^(-(27-n)/2), 6^-10 = 1.7e-8).
+// backward recursion run from n = 32 down to n = 0 (moments_backward_fp32) is
+// accurate to FP32 rounding in every direction, on the source axis included.
 constexpr double kSplitMinNearC = 6.0;
 bool split_supported(int N, int LQ);
 int split_far_chunks(int M, int sm_count);

@@ -224,6 +224,41 @@ def test_exactly_collinear_fibers_report_nan():
         assert e.value.status == 6
 
 
+def test_distant_pair_near_source_axis_mixed_path():
+    """Two fibers 88 half-lengths apart, the target points within 1e-4 of the
+    source fiber's axis (a pair met in a sedimenting cloud).  The reference's
+    closed forms for the n = 0, 1 moments divide differences of O(1) terms by
+    d = c - b^2/4, tiny here: in FP64 they lose all digits of S_1 and the
+    block of this pair comes out as large as its true entries
+    (Int_analytical.f90:162-196).  The mixed path integrates this far pair by
+    the FP32 backward recursion alone, down to n = 0.  Truth: FP64 numeric
+    integration (24-point composite Gauss rule over the source), exact to
+    rounding for a source this far away.  Bound, on the largest deviation
+    relative to the largest entry of A as elsewhere: 1e-8 (the blocks of this
+    pair are 1.7e-7 at most; the FP32 far field deviates by 3e-10)."""
+    p = np.array([0.00162206, 0.0257636, 0.99966675])
+    t = np.array([0.00973097, 0.11302506, -0.99354449])
+    pos = np.array([[0.0, 0.0, 0.0], 88.0 * p + np.array([0.0, 1e-4, 0.0]), [3.0, 0.0, 0.0]])
+    ori = np.array([p, t, [1.0, 0.0, 0.0]])
+    ori /= np.linalg.norm(ori, axis=1, keepdims=True)
+
+    def matrix(**kw):
+        with make_sim(pos, ori, slenderness=1e-3, **kw) as s:
+            s.assemble_system()
+            return s.matrix().astype(np.float64)
+
+    A_num = matrix(use_analytical_integration=0)
+    A_mix = matrix(precision=rf.PREC_MIXED_FP32, velocity_mode=rf.VEL_REUSE)
+    A_64 = matrix()
+    scale = np.abs(A_num).max()
+    n = 15  # 3N rows per fiber
+    for ti, si in ((1, 0), (0, 1)):
+        blk = (slice(n * ti, n * ti + n), slice(n * si, n * si + n))
+        e_mix = np.abs(A_mix[blk] - A_num[blk]).max() / scale
+        e_64 = np.abs(A_64[blk] - A_num[blk]).max() / scale
+        assert e_mix <= 1e-8, (ti, si, e_mix, e_64)
+
+
 def _fp64_reference(pos, ori, eps, tol=1e-12):
     with make_sim(pos, ori, slenderness=eps, gmres_tol=tol, gmres_max_iters=2000) as sim:
         sim.assemble_system()
@@ -332,3 +367,47 @@ def test_checkpoint_resume_matches_uninterrupted(golden):
         got = c.state()
     for g, r in zip(got, ref):
         assert np.abs(g - r).max() <= 1e-11
+
+
+@pytest.mark.parametrize("prec", [rf.PREC_MIXED_BF16, rf.PREC_MIXED_FP32])
+def test_mixed_precision_error_every_step_m2000(prec):
+    """M = 2000 fibers in a cube of side 6.5, 50 steps of the mixed path (BF16
+    or FP32 storage, FP64 refinement to 1e-10).  At every step the velocities
+    and coefficients are compared with an FP64 solve of the same state: the
+    velocity error stays within 1e-6 of the largest velocity over the run.
+    The coefficient bound is looser: the FP32 rounding of A is amplified by the
+    conditioning of the state (fibers of this cloud touch: minimum segment
+    distance 0), and at one step of this run (t = 42, FP32 storage) the FP64
+    solve itself is off by 2e-5: an ejected fiber 88 half-lengths below lies
+    on another fiber's axis, where the reference's closed-form moments lose
+    their digits (test_distant_pair_near_source_axis_mixed_path)."""
+    M, steps = 2000, 50
+    pos, ori = rf.generate_layout(M, "uniform", 6.5, 0.2, seed=1003)
+    mixed = make_sim(pos, ori, slenderness=1e-3, precision=prec, gmres_tol=1e-10, gmres_max_iters=300,
+                     velocity_mode=rf.VEL_REUSE)
+    ref = make_sim(pos, ori, slenderness=1e-3, gmres_tol=1e-12, gmres_max_iters=2000)
+    worst_v, worst_x = 0.0, (0.0, -1)
+    try:
+        for t in range(steps):
+            mixed.assemble_system()
+            assert mixed.solve_system() == 0
+            mixed.update_velocities()
+            V, W = mixed.velocities()
+            x = mixed.coeffs()
+            P, T = mixed.state()
+            ref.set_state(P, T)
+            ref.assemble_system()
+            ref.solve_system()
+            ref.update_velocities()
+            V64, W64 = ref.velocities()
+            x64 = ref.coeffs()
+            ev = max(np.abs(V - V64).max() / np.abs(V64).max(), np.abs(W - W64).max() / np.abs(W64).max())
+            ex = np.abs(x - x64).max() / np.abs(x64).max()
+            worst_v = max(worst_v, ev)
+            worst_x = max(worst_x, (ex, t))
+            assert ev <= 1e-6, (t, ev)
+            mixed.update_fibers(t == 0)
+    finally:
+        mixed.close()
+        ref.close()
+    assert worst_x[0] <= 1e-4, worst_x

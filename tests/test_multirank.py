@@ -1,0 +1,67 @@
+"""bench.py's multi-rank plumbing on CPU: two gloo ranks.
+
+`bench.py --gpus N` runs N independent replicas (one process per GPU, launched
+by torchrun): every rank times its own steps between barriers and the job
+time is the maximum over ranks.  Here two CPU processes stand in for the
+GPUs: the same rendezvous (127.0.0.1), the same barrier and max-over-ranks
+helpers, on the gloo backend, and the reference arm's rule that only rank 0
+works and prints.
+"""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+RANK_CODE = r"""
+import json, os, sys
+sys.path.insert(0, {root!r})
+import bench
+world, rank, local = bench.dist_setup(timeout_s=60)
+bench.barrier(world)
+worst = bench.max_over_ranks(1.5 + rank, world)
+sys.argv = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "0", "--M", "20"]
+ref = None
+if rank != 0:
+    ref = bench.run_reference(bench.parse_args())
+bench.barrier(world)
+import torch.distributed as dist
+backend = dist.get_backend()
+dist.destroy_process_group()
+print(json.dumps({{"rank": rank, "world": world, "max": worst, "backend": backend, "ref": ref}}))
+"""
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_gloo_ranks_barrier_and_max_over_ranks():
+    port = _free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, "-c", RANK_CODE.format(root=ROOT)], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        try:
+            out, err = p.communicate(timeout=180)
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            pytest.fail("a rank did not finish")
+        assert p.returncode == 0, err[-2000:]
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    outs.sort(key=lambda d: d["rank"])
+    for d in outs:
+        assert d["world"] == 2 and d["backend"] == "gloo"
+        assert d["max"] == 2.5  # the slowest rank's time is the job's time
+    assert outs[1]["ref"] is None  # the reference arm runs on rank 0 only
