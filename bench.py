@@ -49,6 +49,26 @@ L2_BYTES = 126 * 1024 * 1024
 # workload's matrix size (the traffic grows with the elements streamed)
 TRAFFIC_PER_ELEMENT = (451.270656e6 + 7.171840e6) / (15040 * 15000)
 
+# The other configurations of the benchmark (seeded synthetic layouts; half
+# length 1, eps 1e-3, N = 5, 8 x 3 Gauss points, gravity (0,0,-1), minimum
+# centre distance 0.2).  Each arm runs the configuration's whole trajectory
+# from the initial layout; the velocity error is taken against an FP64 solve
+# (tol 1e-12) of the same state at the listed steps (1-based).  Arms: (name,
+# precision, GMRES tolerance, preconditioner, velocities).
+CONFIGS = {
+    1: dict(M=100, distribution="uniform", box=2.5, seed=1001, dt=0.1, steps=10, check=(1, 10),
+            arms=[("fp64", "PREC_FP64", 1e-10, "PC_NONE", "VEL_RECOMPUTE")]),
+    2: dict(M=1000, distribution="uniform", box=5.0, seed=1002, dt=0.1, steps=100, check=(1, 50, 100),
+            arms=[("fp64", "PREC_FP64", 1e-10, "PC_NONE", "VEL_RECOMPUTE"),
+                  ("fp32", "PREC_FP32", 1e-5, "PC_NONE", "VEL_RECOMPUTE")]),
+    3: dict(M=2000, distribution="uniform", box=6.5, seed=1003, dt=0.1, steps=50, check=tuple(range(1, 51)),
+            arms=[("bf16+fp64-refine", "PREC_MIXED_BF16", 1e-10, "PC_NONE", "VEL_REUSE"),
+                  ("fp32+fp64-refine", "PREC_MIXED_FP32", 1e-10, "PC_NONE", "VEL_REUSE")]),
+    5: dict(M=8000, distribution="uniform", box=10.0, seed=1005, dt=0.05, steps=100, check=(1, 50, 100),
+            arms=[("bf16+fp64-refine+learned", "PREC_MIXED_BF16", 1e-10, "PC_LEARNED", "VEL_REUSE"),
+                  ("fp32", "PREC_FP32", 1e-5, "PC_NONE", "VEL_RECOMPUTE")]),
+}
+
 
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
@@ -62,6 +82,9 @@ def parse_args():
     ap.add_argument("--weights", default=os.path.join(ROOT, "rigidfibers_kth_b200", "mlp_weights.npy"))
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=4,
+                    help="workload: 4 = the M=4000 benchmark (default); 1, 2, 3, 5 = the other configurations, each "
+                         "run over its whole trajectory from the initial layout (CONFIGS)")
     return ap.parse_args()
 
 
@@ -372,6 +395,136 @@ def run_ours(args):
     return out
 
 
+# ---------------------------------------------------------------- other configurations
+def config_sim(rf, cfg, pos, ori, device, precision, tol, pc, velocity_mode):
+    p = rf.FiberParams(slenderness=1e-3, timestep=cfg["dt"], num_terms_in_force_expansion=5,
+                       num_quadrature_intervals=8, gmres_restart=10, gmres_tol=tol,
+                       gmres_max_iters=300 if tol >= 1e-10 else 2000, precision=precision, preconditioner=pc,
+                       velocity_mode=velocity_mode, device=device)
+    return rf.Simulation(rf.Configuration(p, pos, ori))
+
+
+def run_config(args):
+    """One configuration of the benchmark other than the M=4000 headline: every
+    arm over the whole trajectory (device time of all steps, events on the
+    handle's stream), the roofline of its matrix-vector products (timed live),
+    the velocity error at the configuration's check steps against FP64, and the
+    CPU oracle on the same layout (full steps at M=100, the bounded row sample
+    otherwise)."""
+    world, rank, local = dist_setup()
+    import rigidfibers_kth_b200 as rf
+
+    cfg = CONFIGS[args.config]
+    M, steps = cfg["M"], cfg["steps"]
+    pos, ori = rf.generate_layout(M, cfg["distribution"], cfg["box"], 0.2, seed=cfg["seed"] + rank)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    arms, checks = {}, {}
+    clocks = ClockSampler(local)
+    clocks.start()
+    for name, prec, tol, pc, vel in cfg["arms"]:
+        sim = config_sim(rf, cfg, pos, ori, local, getattr(rf, prec), tol, getattr(rf, pc), getattr(rf, vel))
+        if pc == "PC_LEARNED":
+            sim.set_mlp_weights(np.load(args.weights))
+        barrier(world)
+        sim.gemv_timer(True)
+        launches0 = sim.kernel_launches()
+        total_ms, iters, saved, failed = 0.0, [], [], None
+        for t in range(steps):
+            pre = sim.state() if (t + 1) in cfg["check"] else None
+            sim.mark(0)
+            try:
+                sim.step(t)
+            except rf.RfError as e:  # reported in the arm's entry; the other arms still run
+                failed = f"step {t + 1}: {e}"
+                break
+            sim.mark(1)
+            total_ms += sim.elapsed_ms(0, 1)
+            iters.append(sim.solve_stats()["iterations"])
+            if pre is not None:
+                saved.append((t + 1, pre, sim.velocities()))
+        count, gms, gbytes = sim.gemv_timer(False)
+        launches = sim.kernel_launches() - launches0
+        sim.close()
+        barrier(world)
+        total_ms = max_over_ranks(total_ms, world)
+        per = gms / max(count, 1)
+        ach = gbytes / (per * 1e-3) / 1e9 if count else None
+        done = len(iters)
+        arms[name] = {"value": world * done / (total_ms * 1e-3) if done else None, "unit": "steps/s",
+                      "ms_per_step": total_ms / done if done else None, "steps_completed": done, "failed": failed,
+                      "gmres_tol": tol, "mean_iterations": float(np.mean(iters)) if iters else None,
+                      "gpu_launches": int(launches),
+                      "products": {"bytes": gbytes, "ms_per_launch": per, "launches": count, "achieved_gbs": ach,
+                                   "frac": ach / hbm_peak if ach else None,
+                                   "share_of_run": gms / total_ms if total_ms else None}}
+        checks[name] = saved
+    clk = clocks.stop()
+    # velocity error at the check steps against an FP64 solve of the same state
+    # (after the arms: at M = 8000 the FP64 matrix alone takes 115 GB)
+    ref = config_sim(rf, cfg, pos, ori, local, rf.PREC_FP64, 1e-12, rf.PC_NONE, rf.VEL_RECOMPUTE)
+    for name, saved in checks.items():
+        errs = []
+        for step, (P, T), (V, W) in saved:
+            ref.set_state(P, T)
+            ref.assemble_system()
+            ref.solve_system()
+            ref.update_velocities()
+            V64, W64 = ref.velocities()
+            errs.append((step, float(np.abs(V - V64).max() / np.abs(V64).max()),
+                         float(np.abs(W - W64).max() / np.abs(W64).max())))
+        e = max(errs, key=lambda w: max(w[1], w[2])) if errs else None
+        arms[name]["velocity_error"] = None if e is None else {
+            "steps_checked": [w[0] for w in errs] if len(errs) <= 5 else f"1..{errs[-1][0]}",
+            "worst_step": e[0], "translational": e[1], "rotational": e[2],
+            "norm": "max over fibers / max |FP64 velocity| of the same state"}
+    ref.close()
+    out = None
+    if rank == 0:
+        first = cfg["arms"][0][0]
+        cpu = None
+        if not args.no_cpu:
+            if M <= 100:
+                from oracle import rfo
+
+                o = rfo.Simulation(rfo.make_params(M, eps=1e-3, dt=cfg["dt"], max_iters=300, tol=1e-10), pos, ori)
+                t0 = time.perf_counter()
+                for _ in range(steps):
+                    o.step()
+                cpu_s = (time.perf_counter() - t0) / steps
+                o.close()
+                cpu = {"value": 1.0 / cpu_s, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+                       "sample": f"all {steps} steps of the oracle (FP64, GMRES tol 1e-10)"}
+            else:
+                cpu = cpu_baseline_sample(pos, ori, FP64_MATVECS_PER_STEP)
+        arm = arms[first]
+        prod = arm["products"]
+        out = {
+            "metric": f"steps/s, configuration {args.config} (M={M}): " + " vs ".join(a[0] for a in cfg["arms"]),
+            "value": arm["value"], "unit": "steps/s", "n_gpus": world, "steps": steps, "warmup": 0,
+            "ms_per_step": arm["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": first, "data": "synthetic",
+            "config": {"workload": f"M={M} fibers, centres {cfg['distribution']} in a cube of side {cfg['box']} "
+                                   f"(seed {cfg['seed']}), eps 1e-3, N=5, 8x3 Gauss points, dt {cfg['dt']}, "
+                                   f"{steps} steps from the initial layout",
+                       "timing": "device time of every step of the trajectory, first step included",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": f"matrix-vector products of the {first} arm",
+                         "achieved": prod["achieved_gbs"], "peak": hbm_peak, "unit": "GB/s", "frac": prod["frac"],
+                         "traffic": None,
+                         "peak_source": "measured (copy)" if "hbm_gbs" in peaks else "fallback"},
+            "cpu_baseline": cpu,
+            "arms": arms,
+            "clocks": clk,
+        }
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return out
+
+
 # ---------------------------------------------------------------- reference arm
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -416,7 +569,10 @@ def run_reference(args):
 
 def main():
     args = parse_args()
-    out = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        out = run_reference(args)
+    else:
+        out = run_ours(args) if args.config == 4 else run_config(args)
     if out is not None:
         print(json.dumps(out), flush=True)
 

@@ -510,10 +510,8 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
             for (int q = 0; q < LQ; ++q) {
                 const float sq = s_pv[q];
                 const float r0x = fmaf(sq, t[0], D[0]), r0y = fmaf(sq, t[1], D[1]), r0z = fmaf(sq, t[2], D[2]);
-                const float b = -2.0f * (p[0] * r0x + p[1] * r0y + p[2] * r0z);
-                const float c = r0x * r0x + r0y * r0y + r0z * r0z;
                 float I[KW], J[KW], S[KW];
-                moments_fp32<N, FAR>(b, c, I, J, S);
+                moments_fp32<N, FAR>(Geom32(r0x, r0y, r0z, p[0], p[1], p[2]), I, J, S);
                 const float *w = s_w + q * KW;
                 float wk[KW];
 #pragma unroll

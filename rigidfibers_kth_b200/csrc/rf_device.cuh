@@ -179,34 +179,62 @@ __device__ __forceinline__ void moments_backward_fp32(float b, float c, float *I
     }
 }
 
+// Geometry of one (target point, source fiber) item in FP32 for the moments:
+// b = -2 p.R0, c = |R0|^2, and the three quantities that the closed forms
+// need near the source and that c and b determine only through cancellation:
+// ue^2 = 1 + b + c = |R0 - p|^2, ub^2 = 1 - b + c = |R0 + p|^2 and
+// d = c - b^2/4 = |R0 x p|^2 (|p| = 1).  Formed from the vectors they keep
+// their relative accuracy when a target point comes within 1e-4 of the
+// source fiber (fibers that touch or cross); from b and c they round to zero
+// or below, and the closed forms then take the root or logarithm of a
+// negative number.
+struct Geom32 {
+    float b, c, ue2, ub2, d;
+    __device__ __forceinline__ Geom32(float r0x, float r0y, float r0z, float px, float py, float pz) {
+        b = -2.0f * (px * r0x + py * r0y + pz * r0z);
+        c = r0x * r0x + r0y * r0y + r0z * r0z;
+        const float ex = r0x - px, ey = r0y - py, ez = r0z - pz;
+        const float fx = r0x + px, fy = r0y + py, fz = r0z + pz;
+        ue2 = ex * ex + ey * ey + ez * ez;
+        ub2 = fx * fx + fy * fy + fz * fz;
+        const float cx = fmaf(r0y, pz, -r0z * py), cy = fmaf(r0z, px, -r0x * pz), cz = fmaf(r0x, py, -r0y * px);
+        d = cx * cx + cy * cy + cz * cz;
+    }
+};
+
 // FP32 moments for every point of the plain FP32 method and for the far field
 // (c >= near_c >= 10) of the tile mixed-precision kernel.  For c >= 10 the
-// backward recursion alone (moments_backward_fp32).  Below 10 (plain FP32
-// method only) the reference's closed forms and forward recursion, the closed
+// backward recursion alone (moments_backward_fp32; it needs only b and c).
+// Below 10 (plain FP32 method only) the reference's closed forms and forward
+// recursion on ue^2, ub^2 and d formed from the vectors (Geom32), the closed
 // forms rewritten without the cancellation te/ue - tb/ub (which loses all FP32
 // digits when the target point lies near the source axis):
 // te/ue - tb/ub = 2b d / ((te ub + tb ue) ue ub) when te and tb share a sign.
 // FAR = true: the caller guarantees c >= 6 (far pairs of the split assembly).
 template <int N, bool FAR = false>
-__device__ __forceinline__ void moments_fp32(float b, float c, float *I, float *J, float *S) {
+__device__ __forceinline__ void moments_fp32(const Geom32 &g, float *I, float *J, float *S) {
+    const float b = g.b, c = g.c;
     if (FAR || c >= 10.0f) {
         moments_backward_fp32<N>(b, c, I, J, S);
         return;
     }
     constexpr int K = N + 3;
-    const float ue = sqrtf(1.0f + b + c);
-    const float ub = sqrtf(1.0f - b + c);
+    const float ue = sqrtf(g.ue2);
+    const float ub = sqrtf(g.ub2);
     const float te = 1.0f + 0.5f * b;
     const float tb = -1.0f + 0.5f * b;
-    const float d = c - 0.25f * b * b;
+    const float d = g.d;
     const float iue = __frcp_rn(ue), iub = __frcp_rn(ub), id = __frcp_rn(d);
     // log((2te + 2ue)/(2tb + 2ub)) with the smaller operand formed stably
     const float ae = (te >= 0.f) ? (te + ue) : d * __frcp_rn(ue - te);
     const float ab = (tb >= 0.f) ? (tb + ub) : d * __frcp_rn(ub - tb);
     I[0] = logf(ae * __frcp_rn(ab));
     I[1] = ue - ub - 0.5f * b * I[0];
-    if (d < 1e-6f * c) {
-        // point on the source axis: the d -> 0 limits (Int_analytical.f90:162-164, 189-191)
+    if (d < 1e-6f * c && te * tb > 0.f) {
+        // point on the source axis beyond its ends: the d -> 0 limits
+        // (Int_analytical.f90:162-164, 189-191).  Within the span (te tb < 0:
+        // fibers that touch or cross) the general forms below hold with the
+        // accurate d and have no cancellation.
         J[0] = 0.5f * (__frcp_rn(tb * tb) - __frcp_rn(te * te));
         J[1] = -iue + iub - 0.5f * b * J[0];
         const float p = 2.0f + b, m = -2.0f + b;
@@ -375,9 +403,7 @@ template <int N>
 __device__ __forceinline__ void inner_analytic_store_fp32(float r0x, float r0y, float r0z, float px, float py,
                                                           float pz, float eps2, double *dst, int ld) {
     float I[N + 3], J[N + 3], S[N + 3];
-    const float b = -2.0f * (px * r0x + py * r0y + pz * r0z);
-    const float c = r0x * r0x + r0y * r0y + r0z * r0z;
-    moments_fp32<N>(b, c, I, J, S);
+    moments_fp32<N>(Geom32(r0x, r0y, r0z, px, py, pz), I, J, S);
     const Outer<float> o(r0x, r0y, r0z, px, py, pz);
     GStore<float, N>::run(I, J, S, o, eps2, dst, ld);
 }
@@ -398,9 +424,7 @@ template <int N>
 __device__ __forceinline__ void inner_analytic_fp32(float r0x, float r0y, float r0z, float px, float py,
                                                     float pz, float eps2, float (*G)[6]) {
     float I[N + 3], J[N + 3], S[N + 3];
-    const float b = -2.0f * (px * r0x + py * r0y + pz * r0z);
-    const float c = r0x * r0x + r0y * r0y + r0z * r0z;
-    moments_fp32<N>(b, c, I, J, S);
+    moments_fp32<N>(Geom32(r0x, r0y, r0z, px, py, pz), I, J, S);
     const Outer<float> o(r0x, r0y, r0z, px, py, pz);
     GAll<float, N>::run(I, J, S, o, eps2, G);
 }
