@@ -96,7 +96,10 @@ typedef struct rf_params {
     int32_t device;                      /* CUDA device ordinal */
     int32_t max_refinements;             /* mixed precision: outer refinement steps (default 30) */
     int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 12) */
-    double inner_tol;                    /* mixed precision: inner GMRES relative tolerance (default 3e-3) */
+    double inner_tol;                    /* mixed precision: the deepest reduction one inner GMRES solve
+                                            is asked for (default 1e-3); the refinements are planned as the
+                                            fewest that reach gmres_tol with inner solves no deeper than
+                                            this, each asking for an equal share of what is still needed */
     double near_field_c;                 /* mixed precision: squared distance below which the analytic
                                             integral stays FP64 (default 6: from there on the FP32
                                             backward recursion reaches FP32 accuracy; raised to 10

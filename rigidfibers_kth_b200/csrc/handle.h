@@ -95,6 +95,7 @@ struct rf_handle {
     } gt;
 
     rf_solve_stats stats{};
+    int cold_solves = 0;  // mixed solves left that start from zero (poor warm start seen)
     bool assembled = false;
     int64_t launches = 0;
     std::string err;

@@ -43,7 +43,7 @@ class FiberParams:
     device: int = 0
     max_refinements: int = 30
     cluster_size: int = 12
-    inner_tol: float = 3e-3
+    inner_tol: float = 1e-3
     near_field_c: float = 6.0
 
     def to_c(self):
