@@ -30,9 +30,10 @@ and writes the trajectory and the per-step dumps.  Outputs, all optional:
                    (filename3 is never renamed), the coefficient file rolls
                    over with the other two.
 
-The parameter file's GMRES settings apply.  A file that asks for the direct
-solver (line 11 = 1) is solved by GMRES to 1e-13, which agrees with the LU
-solution far below the printed precision; the dense LU path is not built.
+The parameter file's solver settings apply: GMRES, or the device LU when
+line 11 asks for the direct solver.  The LU is FP64 only; with a mixed or
+FP32 precision a direct request is solved by GMRES to 1e-13 instead (which
+agrees with the LU solution far below the printed precision).
 """
 import argparse
 import os
@@ -181,12 +182,12 @@ def configuration(args):
     M, pos, ori = parse_layout_file(args.layout)
     params.num_fibers = M
     notes = []
-    if params.use_direct_solver:
+    params.precision = PRECISIONS[args.precision]
+    if params.use_direct_solver and params.precision != L.PREC_FP64:
         params.use_direct_solver = 0
         params.gmres_tol = min(params.gmres_tol, 1e-13)
         params.gmres_max_iters = max(params.gmres_max_iters, 1000)
-        notes.append("direct solver requested: solved by GMRES to 1e-13 (the dense LU path is not built)")
-    params.precision = PRECISIONS[args.precision]
+        notes.append("direct solver requested with a reduced precision: solved by GMRES to 1e-13 (the LU is FP64 only)")
     params.preconditioner = PRECONDITIONERS[args.preconditioner]
     params.velocity_mode = VELOCITY_MODES[args.velocities]
     params.device = args.device

@@ -3,6 +3,7 @@
 // assemble_system -> solve_system -> update_velocities -> update_fibers.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <string>
 
@@ -30,7 +31,7 @@ void free_all(rf_handle *h) {
         cudaFree(h->V[i]);
         cudaFree(h->W[i]);
     }
-    void *ptrs[] = {h->tab, h->A64, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
+    void *ptrs[] = {h->tab, h->A64, h->LU, h->lu_r, h->lu_piv, h->lu_info, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
                     h->PV32, h->PW32, h->vpart, h->pvx, h->pwx, h->work64, h->work32, h->r64, h->r32,
                     h->d32, h->x32, h->Pblocks, h->knn, h->mlp_w, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out,
                     h->dscal, h->rb.partials, h->rb.counter, h->near_bits, h->near_list, h->near_cnt,
@@ -258,8 +259,8 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown preconditioner");
     if (p->velocity_mode != RF_VEL_RECOMPUTE && p->velocity_mode != RF_VEL_REUSE)
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown velocity mode");
-    if (p->use_direct_solver)
-        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "use_direct_solver: the dense LU path is not built; use GMRES");
+    if (p->use_direct_solver && p->precision != RF_PREC_FP64)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "use_direct_solver needs precision RF_PREC_FP64");
     if (p->gmres_restart < 1 || p->gmres_restart > 64 || !(p->gmres_tol > 0.0))
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "gmres_restart must be 1..64 and gmres_tol > 0");
     if (!finite_all(positions, 3 * (size_t)M) || !finite_all(orientations, 3 * (size_t)M))
@@ -603,7 +604,45 @@ rf_status rf_solve_system(rf_handle *h) {
     const int nb = 3 * h->N;
     rf::GmresResult res;
     rf_status status = RF_OK;
-    if (prec == RF_PREC_FP64) {
+    if (prec == RF_PREC_FP64 && h->p.use_direct_solver) {
+        // dgesv (coeffs_and_vels.f90:62,158): LU factors of a copy of A (A
+        // itself stays available to rf_get_matrix and rf_matvec), then the two
+        // triangular solves; the factors' buffer is made at the first call
+        const size_t mat = sizeof(double) * (size_t)h->lda * (size_t)h->n;
+        if (!h->LU) {
+            CK(h, cudaMalloc(&h->LU, mat), "direct solver: LU factors (one more n x n FP64 matrix)");
+            CK(h, cudaMalloc(&h->lu_r, sizeof(double) * h->n), "direct solver");
+            CK(h, cudaMalloc(&h->lu_piv, sizeof(int) * h->n), "direct solver");
+            CK(h, cudaMalloc(&h->lu_info, sizeof(int)), "direct solver");
+        }
+        CK(h, cudaMemcpyAsync(h->LU, h->A64, mat, cudaMemcpyDeviceToDevice, st), "direct solver");
+        CK(h, cudaMemcpyAsync(h->x, h->b, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, st), "direct solver");
+        CK(h, rf::lu_factor(h->LU, h->lda, h->n, h->lu_piv, h->lu_info, st, &h->launches), "LU factorisation");
+        CK(h, rf::lu_solve(h->LU, h->lda, h->n, h->lu_piv, h->x, st, &h->launches), "LU solve");
+        // backward error |b - A x| / |b| for the statistics
+        CK(h, (rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, h->x, h->lu_r, h->b,
+                                                                h->work64, h->work_elems, h->sm_count, st)),
+           "direct solver residual");
+        CK(h, rf::launch_dot<double>(h->n, h->lu_r, h->lu_r, h->dscal, h->rb, st), "direct solver residual");
+        CK(h, rf::launch_dot<double>(h->n, h->b, h->b, h->dscal + 1, h->rb, st), "direct solver residual");
+        h->launches += 4;
+        int *hinfo = reinterpret_cast<int *>(h->hscal + 7);
+        CK(h, cudaMemcpyAsync(h->hscal, h->dscal, 2 * sizeof(double), cudaMemcpyDeviceToHost, st), "direct solver");
+        CK(h, cudaMemcpyAsync(hinfo, h->lu_info, sizeof(int), cudaMemcpyDeviceToHost, st), "direct solver");
+        CK(h, cudaStreamSynchronize(st), "direct solver");
+        const double rr = h->hscal[0], bb = h->hscal[1];
+        if (!(std::isfinite(rr) && std::isfinite(bb)) && *hinfo == 0)
+            return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
+        h->stats.iterations = 0;
+        h->stats.matvecs = 1;
+        h->stats.residual = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+        h->stats.converged = *hinfo == 0;
+        if (*hinfo != 0) {
+            char msg[96];
+            std::snprintf(msg, sizeof(msg), "singular matrix: LU pivot %d is zero", *hinfo);
+            return rf::fail(h, RF_ERR_NOT_CONVERGED, msg);
+        }
+    } else if (prec == RF_PREC_FP64) {
         rf::Gmres<double>::Op A = [h](const double *in, double *out) {
             h->launches += 2;
             return timed_product(h, 8.0 * h->lda * h->n, [&] {

@@ -37,6 +37,10 @@ struct rf_handle {
     rf::Tables tab_h{};
     rf::Tables *tab = nullptr;
     double *A64 = nullptr;
+    double *LU = nullptr;      // direct solver: LU factors of A64 (ld lda), made at the first direct solve
+    double *lu_r = nullptr;    // direct solver: residual b - A x for the statistics
+    int *lu_piv = nullptr;     // [n] pivot rows
+    int *lu_info = nullptr;
     float *A32 = nullptr;
     __nv_bfloat16 *A16 = nullptr;
     double *b = nullptr;       // right-hand side

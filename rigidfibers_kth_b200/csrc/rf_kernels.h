@@ -127,6 +127,14 @@ cudaError_t launch_mgs_norm(int64_t n, T *w, const T *vprev, const double *hprev
 // out = dot(a, b) (double accumulation)
 template <typename T>
 cudaError_t launch_dot(int64_t n, const T *a, const T *b, double *out, const RedBuf &rb, cudaStream_t st);
+
+// Direct solve (lu.cu): A (n x n, column-major, ld lda) is overwritten by its
+// LU factors with partial pivoting, piv[n] the pivot rows (0-based), info the
+// first zero pivot (1-based) or 0; lu_solve overwrites x (= b on entry) with
+// the solution.  launches counts the kernels launched.
+cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, cudaStream_t st, int64_t *launches);
+cudaError_t lu_solve(const double *A, int64_t lda, int64_t n, const int *piv, double *x, cudaStream_t st,
+                     int64_t *launches);
 // y = alpha_scale * x where alpha_scale = num/den (den device scalar), i.e. y = x * (num / *den)
 template <typename TO, typename TI>
 cudaError_t launch_scale(int64_t n, const TI *x, const double *den, double num, TO *y, cudaStream_t st);

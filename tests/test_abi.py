@@ -92,6 +92,15 @@ def test_parameter_and_layout_files(tmp_path):
     assert cfg.parameters.num_fibers == 7
 
 
+def test_direct_solver_needs_fp64():
+    """The device LU is FP64 only: asking for it with a mixed precision is
+    rejected before any device work (no GPU needed)."""
+    pos, ori = rf.generate_layout(4, "uniform", 3.0, 0.2, seed=1)
+    with pytest.raises(rf.RfError) as e:
+        rf.Simulation(rf.Configuration(rf.FiberParams(use_direct_solver=1, precision=rf.PREC_MIXED_BF16), pos, ori))
+    assert e.value.status == 1 and "RF_PREC_FP64" in str(e.value)
+
+
 def test_create_without_gpu_fails_cleanly():
     from conftest import gpu_available
 

@@ -57,14 +57,11 @@ def test_assembly_matches_oracle_fp64(golden, analytic):
 
 @pytest.mark.parametrize("case", [c for c in CASES])
 def test_two_steps_match_golden(golden, case):
-    """The golden vectors of all four reference runs.  The direct-solver cases
-    are reproduced with GMRES at tol 1e-13 (LU and tight GMRES agree far below
-    the printed precision)."""
+    """The golden vectors of all four reference runs, the direct-solver cases
+    through the device LU (dgesv in the reference)."""
     X0, T0 = golden["layout_pos"], golden["layout_orient"]
-    tol = 1e-13 if "direct" in case else 1e-5
-    maxit = 1000 if "direct" in case else 100
-    with make_sim(X0, T0, use_analytical_integration=int("analytic" in case), gmres_tol=tol,
-                  gmres_max_iters=maxit) as sim:
+    with make_sim(X0, T0, use_analytical_integration=int("analytic" in case),
+                  use_direct_solver=int("direct" in case)) as sim:
         for step in (0, 1):
             sim.assemble_system()
             b = sim.rhs()
@@ -78,6 +75,43 @@ def test_two_steps_match_golden(golden, case):
             for q in QUANTITIES:
                 err = np.abs(out[q] - golden[f"{case}/{step}_{q}"]).max()
                 assert err <= GOLDEN_ATOL, (case, step, q, err)
+
+
+@pytest.mark.parametrize("M", [100, 300])
+def test_direct_solver_matches_oracle_lu(M):
+    """Device LU with partial pivoting (panels of 32; n = 1500 and 4500, the
+    last panel partial) against the oracle's LU (LAPACK dgesv's algorithm) of
+    the same matrix: coefficients within 1e-10, the device's backward error at
+    rounding level, and A left in place (the factors have their own buffer)."""
+    pos, ori = rf.generate_layout(M, "uniform", 5.0 * (M / 300) ** (1 / 3), 0.2, seed=1900 + M)
+    with make_sim(pos, ori, slenderness=1e-3, use_direct_solver=1) as sim:
+        sim.assemble_system()
+        A0 = sim.matrix()
+        b = sim.rhs()
+        assert sim.solve_system() == 0
+        x = sim.coeffs()
+        st = sim.solve_stats()
+        A1 = sim.matrix()
+        y = sim.matvec(x)
+    assert st["converged"] and st["iterations"] == 0
+    assert st["residual"] <= 1e-13
+    assert np.linalg.norm(y - b) / np.linalg.norm(b) <= 1e-13
+    assert np.array_equal(A0, A1)
+    x_o = rfo.solve_direct(A0, b)
+    assert np.abs(x - x_o).max() <= 1e-10 * np.abs(x_o).max()
+
+
+def test_direct_solver_steps_match_gmres():
+    """Three time steps with the LU and with GMRES at 1e-13 agree."""
+    pos, ori = rf.generate_layout(200, "uniform", 4.0, 0.2, seed=1950)
+    out = []
+    for kw in (dict(use_direct_solver=1), dict(gmres_tol=1e-13, gmres_max_iters=2000)):
+        with make_sim(pos, ori, slenderness=1e-3, **kw) as sim:
+            for t in range(3):
+                sim.step(t)
+            out.append(sim.state() + sim.velocities())
+    for a, b in zip(*out):
+        assert np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(b).max())
 
 
 def test_gmres_iterates_match_oracle(golden):
