@@ -163,6 +163,10 @@ __device__ __forceinline__ void moments_backward_fp32(float b, float c, float *I
     const float icb = ic * b;
     const float icwp = __fdividef(2.0f * b, ue + ub) * ic;  // (ue - ub) / c
     const float icwm = (ue + ub) * ic;
+    const float nic = -ic, nicb = -icb, ic2 = ic * ic;
+    // J and S are carried as c J_n and c^2 S_n: their steps become two fused
+    // multiply-adds each, c J_n = I_n - (b/c) c J_{n+1} - (1/c) c J_{n+2} and
+    // c^2 S_n = c J_n - (b/c) c^2 S_{n+1} - (1/c) c^2 S_{n+2}
     float i1 = 0.f, i2 = 0.f, j1 = 0.f, j2 = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll
     for (int n = kBackTop; n >= 0; --n) {
@@ -172,9 +176,9 @@ __device__ __forceinline__ void moments_backward_fp32(float b, float c, float *I
         const float cb = (1.0f - 2.0f * (n + 2.0f)) / (2.0f * (n + 2.0f));
         const float icw = ((n + 1) % 2 == 0) ? icwp : icwm;
         const float in = fmaf((a0 * cb) * icb, i1, fmaf(-a0 * ic, i2, (a0 * r2) * icw));
-        const float jn = fmaf(ic, in, fmaf(-icb, j1, -ic * j2));
-        const float sn = fmaf(ic, jn, fmaf(-icb, s1, -ic * s2));
-        if (n < K) { I[n] = in; J[n] = jn; S[n] = sn; }
+        const float jn = fmaf(nicb, j1, fmaf(nic, j2, in));
+        const float sn = fmaf(nicb, s1, fmaf(nic, s2, jn));
+        if (n < K) { I[n] = in; J[n] = jn * ic; S[n] = sn * ic2; }
         i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
     }
 }
