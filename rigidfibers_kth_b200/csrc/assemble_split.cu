@@ -270,16 +270,27 @@ __constant__ float c_leg32[8][8] = {{RF_LEG_ROW(0)}, {RF_LEG_ROW(1)}, {RF_LEG_RO
 #ifndef RF_FAR_MINB
 #define RF_FAR_MINB 8
 #endif
+// Warps per far-pair CTA.  Each warp works on its own 32 targets; the warps
+// of a CTA step through the sources together (a barrier before each source's
+// post-processing), so the warps sharing a scheduler mostly run the same code
+// at the same time and share the instruction cache: the Gauss-point loop and
+// the post-processing together exceed it, and warps of separate one-warp CTAs
+// drift into different phases.  Measured at M = 4000: assembly 20.35 ms with
+// one-warp CTAs, 19.5 ms with barriers before both phases, 19.35 ms with the
+// one before the post-processing alone.
+#ifndef RF_FAR_WARPS
+#define RF_FAR_WARPS 8
+#endif
 
 template <int N, bool PANELS>
 struct FarSmem {
     static constexpr int GR = 32 * 3 * N;                   // staged rows of one column
     static constexpr int PAN = 2 * 3 * 96;                  // staged panel columns
     static constexpr int SET = (N + 1) * 7 * 32;            // coefficient sets of one weight [k][7][lane]
-    static size_t bytes() {
-        return sizeof(float) * (32 * kNearWeight + SET + 16 + 64 + kMaxLQ + kMaxLQ * SplitDims<N>::KW + 3 * GR +
-                                (PANELS ? PAN : 0));
-    }
+    static constexpr size_t kBytes = sizeof(float) * (32 * kNearWeight + SET + 16 + 64 + kMaxLQ +
+                                                      kMaxLQ * SplitDims<N>::KW + 3 * GR + (PANELS ? PAN : 0));
+    static_assert(kBytes % 16 == 0, "each warp's region starts on a 16-byte boundary");
+    static size_t bytes() { return kBytes; }
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -398,12 +409,13 @@ __device__ __forceinline__ void far_xyz(const float *o, const float *D, const fl
 }
 
 template <int N, bool PANELS, bool FAR>
-__global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a) {
+__global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS) far_pairs_kernel(SplitArgs a) {
     using SD = SplitDims<N>;
     using SM = FarSmem<N, PANELS>;
     constexpr int NL = SD::NL, NV = SD::NV, KW = SD::KW, NRHS = SD::NRHS, RB = SD::RB, GR = SM::GR;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int lane = threadIdx.x;
+    extern __shared__ __align__(16) unsigned char smem_all[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned char *smem_raw = smem_all + (size_t)warp * SM::kBytes;  // this warp's region
     float *s_nb = reinterpret_cast<float *>(smem_raw);               // [near lane][kNearWeight], one weight
     float *s_set = s_nb + 32 * kNearWeight;                           // [k][7][32]
     float *s_gk = s_set + SM::SET;                                    // gamma_k (0..7), E_k (8..15)
@@ -434,11 +446,11 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
     const float f[3] = {(float)tab.half_force[0], (float)tab.half_force[1], (float)tab.half_force[2]};
     const float e2 = (float)(2.0 * tab.eps2), e6 = (float)(6.0 * tab.eps2);
 
-    const int i0 = blockIdx.x * 32;
+    const int i0 = (blockIdx.x * RF_FAR_WARPS + warp) * 32;
     const int i = i0 + lane;
     const bool valid = i < a.M;
-    const int nvalid = min(32, a.M - i0);
-    const int ic = valid ? i : i0;
+    const int nvalid = min(32, a.M - i0);     // <= 0 for a warp past the last target: it only keeps step
+    const int ic = valid ? i : min(i0, a.M - 1);
     const double xi0 = a.pos[3 * ic], xi1 = a.pos[3 * ic + 1], xi2 = a.pos[3 * ic + 2];
     const float t[3] = {(float)a.ori[3 * ic], (float)a.ori[3 * ic + 1], (float)a.ori[3 * ic + 2]};
     const float tt = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
@@ -534,7 +546,7 @@ __global__ void __launch_bounds__(32, RF_FAR_MINB) far_pairs_kernel(SplitArgs a)
         const float Dt = D[0] * t[0] + D[1] * t[1] + D[2] * t[2];
         const float pt = p[0] * t[0] + p[1] * t[1] + p[2] * t[2];
         cp_async_wait_all();
-        __syncwarp();
+        __syncthreads();  // the CTA's warps enter each source's post-processing together
 
         if (act) {
             // right-hand side: theta^k_0 f for weight 0 (near pairs add theirs in the near kernel)
@@ -921,12 +933,13 @@ __global__ void split_finish_kernel(SplitArgs a, int nchunks, double *b, double 
 
 template <int N, bool PANELS, bool FAR>
 cudaError_t launch_far_n(const SplitArgs &a, int far_chunks, cudaStream_t st) {
-    const size_t smem = FarSmem<N, PANELS>::bytes();
+    const size_t smem = RF_FAR_WARPS * FarSmem<N, PANELS>::bytes();
     auto kern = far_pairs_kernel<N, PANELS, FAR>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    dim3 grid((a.M + 31) / 32, far_chunks);
-    kern<<<grid, 32, smem, st>>>(a);
+    const int groups = (a.M + 31) / 32;
+    dim3 grid((groups + RF_FAR_WARPS - 1) / RF_FAR_WARPS, far_chunks);
+    kern<<<grid, 32 * RF_FAR_WARPS, smem, st>>>(a);
     return cudaGetLastError();
 }
 
