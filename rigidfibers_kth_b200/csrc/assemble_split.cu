@@ -519,6 +519,9 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
 #pragma unroll
             for (int k = 0; k < KW; ++k) V[pp][k] = 0.f;
         if (act) {
+            // two Gauss points in flight (two independent recursions): 2 % faster
+            // once the warps of a scheduler share the instruction stream
+#pragma unroll 2
             for (int q = 0; q < LQ; ++q) {
                 const float sq = s_pv[q];
                 const float r0x = fmaf(sq, t[0], D[0]), r0y = fmaf(sq, t[1], D[1]), r0z = fmaf(sq, t[2], D[2]);
