@@ -287,8 +287,10 @@ struct FarSmem {
     static constexpr int GR = 32 * 3 * N;                   // staged rows of one column
     static constexpr int PAN = 2 * 3 * 96;                  // staged panel columns
     static constexpr int SET = (N + 1) * 7 * 32;            // coefficient sets of one weight [k][7][lane]
+    static constexpr int STG16 = 3 * GR / 2;                // BF16 copy of the staged columns (in floats)
     static constexpr size_t kBytes = sizeof(float) * (32 * kNearWeight + SET + 16 + 64 + kMaxLQ +
-                                                      kMaxLQ * SplitDims<N>::KW + 3 * GR + (PANELS ? PAN : 0));
+                                                      kMaxLQ * SplitDims<N>::KW + 3 * GR + (PANELS ? PAN : 0) +
+                                                      STG16);
     static_assert(kBytes % 16 == 0, "each warp's region starts on a 16-byte boundary");
     static size_t bytes() { return kBytes; }
 };
@@ -298,40 +300,71 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+// Bulk asynchronous shared -> global copies (the copy engine streams staged
+// columns out while the warp goes on computing).  Addresses and sizes are
+// multiples of 16 bytes.
+__device__ __forceinline__ void bulk_s2g(void *gdst, const void *ssrc, unsigned bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(ssrc);
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gdst), "r"(s), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the staged data has been read out: the staging buffers may be rewritten
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+// generic-proxy shared-memory writes made visible to the bulk copies
+__device__ __forceinline__ void fence_async_shared() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <int N, bool PANELS>
 __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, int i0, int nvalid, const float *stg,
-                                            const float *pan, int lane) {
+                                            const float *pan, __nv_bfloat16 *stg16, int lane) {
     constexpr int RB = 3 * N, GR = 32 * RB;
     const int64_t row0 = (int64_t)i0 * RB;
     const int nrows = nvalid * RB;
-#pragma unroll
-    for (int bb = 0; bb < 3; ++bb) {
-        const int64_t col = (int64_t)j * RB + 3 * (m - 1) + bb;
-        const float *src = stg + bb * GR;
-        if (nrows == GR) {
-            const float4 *s4 = reinterpret_cast<const float4 *>(src);
-            if (a.A32) {
-                float4 *d4 = reinterpret_cast<float4 *>(a.A32 + col * a.lda + row0);
-                for (int e = lane; e < GR / 4; e += 32) d4[e] = s4[e];
+    const int64_t col0 = (int64_t)j * RB + 3 * (m - 1);
+    if (nrows == GR) {
+        // whole column segments: the BF16 copy is staged too, then one lane
+        // hands every segment to the copy engine (A32 and A16: 3 x 32 targets
+        // x 3N rows; panels: 2 x 3 x 96 rows), and the warp moves on
+        if (a.A16) {
+            const float4 *s4 = reinterpret_cast<const float4 *>(stg);
+            uint2 *d2 = reinterpret_cast<uint2 *>(stg16);
+            for (int e = lane; e < 3 * GR / 4; e += 32) {
+                const float4 v = s4[e];
+                __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+                uint2 u;
+                u.x = *reinterpret_cast<unsigned *>(&lo);
+                u.y = *reinterpret_cast<unsigned *>(&hi);
+                d2[e] = u;
             }
-            if (a.A16) {
-                uint2 *d2 = reinterpret_cast<uint2 *>(a.A16 + col * a.lda + row0);
-                for (int e = lane; e < GR / 4; e += 32) {
-                    const float4 v = s4[e];
-                    __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
-                    uint2 u;
-                    u.x = *reinterpret_cast<unsigned *>(&lo);
-                    u.y = *reinterpret_cast<unsigned *>(&hi);
-                    d2[e] = u;
+        }
+        fence_async_shared();
+        __syncwarp();
+        if (lane == 0) {
+#pragma unroll
+            for (int bb = 0; bb < 3; ++bb) {
+                const int64_t col = col0 + bb;
+                if (a.A32) bulk_s2g(a.A32 + col * a.lda + row0, stg + bb * GR, GR * sizeof(float));
+                if (a.A16) bulk_s2g(a.A16 + col * a.lda + row0, stg16 + bb * GR, GR * sizeof(__nv_bfloat16));
+                if (PANELS) {
+#pragma unroll
+                    for (int w = 0; w < 2; ++w)
+                        bulk_s2g((w ? a.PW32 : a.PV32) + col * a.ldp + (int64_t)i0 * 3, pan + (w * 3 + bb) * 96,
+                                 96 * sizeof(float));
                 }
             }
-        } else {
-            for (int e = lane; e < nrows; e += 32) {
-                if (a.A32) a.A32[col * a.lda + row0 + e] = src[e];
-                if (a.A16) a.A16[col * a.lda + row0 + e] = __float2bfloat16_rn(src[e]);
-            }
+            bulk_commit();
+        }
+        return;
+    }
+#pragma unroll
+    for (int bb = 0; bb < 3; ++bb) {
+        const int64_t col = col0 + bb;
+        const float *src = stg + bb * GR;
+        for (int e = lane; e < nrows; e += 32) {
+            if (a.A32) a.A32[col * a.lda + row0 + e] = src[e];
+            if (a.A16) a.A16[col * a.lda + row0 + e] = __float2bfloat16_rn(src[e]);
         }
         if (PANELS) {
             const int prow = 3 * nvalid;
@@ -339,11 +372,7 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
             for (int w = 0; w < 2; ++w) {
                 float *dst = (w ? a.PW32 : a.PV32) + col * a.ldp + (int64_t)i0 * 3;
                 const float *ps = pan + (w * 3 + bb) * 96;
-                if (prow == 96) {
-                    if (lane < 24) reinterpret_cast<float4 *>(dst)[lane] = reinterpret_cast<const float4 *>(ps)[lane];
-                } else {
-                    for (int e = lane; e < prow; e += 32) dst[e] = ps[e];
-                }
+                for (int e = lane; e < prow; e += 32) dst[e] = ps[e];
             }
         }
     }
@@ -425,6 +454,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
     float *s_w = s_pv + kMaxLQ;                                       // [kMaxLQ][KW]: w_q P_k(s_q)
     float *s_stg = s_w + kMaxLQ * KW;                                 // [3][GR]
     float *s_pan = s_stg + 3 * GR;                                    // [2][3][96]
+    __nv_bfloat16 *s_stg16 = reinterpret_cast<__nv_bfloat16 *>(s_pan + (PANELS ? SM::PAN : 0));  // [3][GR]
 
     const Tables &tab = *a.tab;
     const int LQ = a.LQ;
@@ -591,6 +621,9 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
 #pragma unroll 1
         for (int it = 0; it < N; ++it) {
             const int m = it < (N + 1) / 2 ? 2 * it + 1 : 2 * (it - (N + 1) / 2) + 2;
+            // the copy engine has read the previous weight's staged columns
+            if (lane == 0) bulk_wait_read();
+            __syncwarp();
             if (m & 1) far_sets<N, 1>(m, U, V, s_set, lane);
             else far_sets<N, 0>(m, U, V, s_set, lane);
             const float *o = s_set + lane;
@@ -670,7 +703,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
                 }
                 cp_async_commit();
             }
-            far_store_m<N, PANELS>(a, m, j, i0, nvalid, s_stg, s_pan, lane);
+            far_store_m<N, PANELS>(a, m, j, i0, nvalid, s_stg, s_pan, s_stg16, lane);
             __syncwarp();
         }
     }
@@ -678,6 +711,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
 #pragma unroll
         for (int r = 0; r < NRHS; ++r) a.far_contr[((int64_t)blockIdx.y * a.M + i) * NRHS + r] = rhs[r];
     }
+    if (lane == 0) bulk_wait_all();  // every staged segment written before the CTA's shared memory goes
 }
 
 // ---------------------------------------------------------------- near pairs (FP64)
