@@ -247,7 +247,7 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
     *out = nullptr;
     if (!p || !positions || !orientations) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "null argument");
     const int M = p->num_fibers, N = p->num_terms_in_force_expansion, NoQI = p->num_quadrature_intervals;
-    if (M < 2) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_fibers must be >= 2");
+    if (M < 1) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_fibers must be >= 1");
     if (N < 1 || N > rf::kMaxN) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_terms_in_force_expansion must be 1..8");
     if (NoQI < 1 || 3 * NoQI > rf::kMaxLQ)
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "num_quadrature_intervals must be 1..16");
@@ -259,6 +259,8 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown preconditioner");
     if (p->velocity_mode != RF_VEL_RECOMPUTE && p->velocity_mode != RF_VEL_REUSE)
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown velocity mode");
+    if (M < 2 && p->preconditioner != RF_PC_NONE)
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "a block preconditioner needs at least two fibers");
     if (p->use_direct_solver && p->precision != RF_PREC_FP64)
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "use_direct_solver needs precision RF_PREC_FP64");
     if (p->gmres_restart < 1 || p->gmres_restart > 64 || !(p->gmres_tol > 0.0))

@@ -44,9 +44,13 @@ def test_create_rejects_bad_arguments():
     nanpos = pos.copy()
     nanpos[0] = np.nan
     assert lib.rf_create(ctypes.byref(p), _ptr(nanpos), _ptr(ori), ctypes.byref(h)) == 6
-    q = rf.FiberParams(num_fibers=1).to_c()
+    q = rf.FiberParams(num_fibers=0).to_c()
     assert lib.rf_create(ctypes.byref(q), _ptr(pos), _ptr(ori), ctypes.byref(h)) == 1
     assert b"num_fibers" in lib.rf_last_error(None)
+    # one fiber is a valid system, but a block preconditioner needs neighbours
+    q = rf.FiberParams(num_fibers=1, preconditioner=rf.PC_LEARNED).to_c()
+    assert lib.rf_create(ctypes.byref(q), _ptr(pos), _ptr(ori), ctypes.byref(h)) == 1
+    assert b"two fibers" in lib.rf_last_error(None)
 
 
 def test_generator_deterministic_and_spaced():

@@ -114,6 +114,37 @@ def test_direct_solver_steps_match_gmres():
         assert np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(b).max())
 
 
+@pytest.mark.parametrize("layout", ["one", "near pair", "far pair"])
+@pytest.mark.parametrize("path", ["fp64", "direct", "fp32", "mixed-bf16", "mixed-fp32"])
+def test_one_and_two_fibers_every_path(layout, path):
+    """The smallest systems through every solver path (one fiber: A = I,
+    b = 0, only the local velocity term; two fibers 0.5 or 8 apart: one near
+    or one far pair, a CTA whose other warps hold no target), two steps,
+    against the oracle's velocities and positions of the same steps."""
+    pos = {"one": [[0.0, 0.0, 0.0]], "near pair": [[0.0, 0.0, 0.0], [0.5, 0.1, 0.0]],
+           "far pair": [[0.0, 0.0, 0.0], [8.0, 1.0, -2.0]]}[layout]
+    ori = [[0.0, 0.6, 0.8], [1.0, 0.0, 0.0]][: len(pos)]
+    pos, ori = np.array(pos), np.array(ori)
+    kw = {"fp64": dict(gmres_tol=1e-13, gmres_max_iters=500), "direct": dict(use_direct_solver=1),
+          "fp32": dict(precision=rf.PREC_FP32, gmres_tol=1e-6),
+          "mixed-bf16": dict(precision=rf.PREC_MIXED_BF16, gmres_tol=1e-12, velocity_mode=rf.VEL_REUSE),
+          "mixed-fp32": dict(precision=rf.PREC_MIXED_FP32, gmres_tol=1e-12)}[path]
+    M = len(pos)
+    o = rfo.Simulation(rfo.make_params(M, eps=1e-3, tol=1e-13, max_iters=500), pos, ori)
+    tol = {"fp64": 1e-10, "direct": 1e-10, "fp32": 1e-4}.get(path, 1e-6)
+    with make_sim(pos, ori, slenderness=1e-3, **kw) as sim:
+        for t in range(2):
+            assert sim.step(t) == 0
+            o.step()
+            ref = o.last()
+            V, W = sim.velocities()
+            P, T = sim.state()
+            for got, want in ((V, ref["TRANSVel"]), (W, ref["ROTVel"]), (P, ref["POS"]), (T, ref["ORIENT"])):
+                assert np.isfinite(got).all()
+                assert np.abs(got - want).max() <= tol * max(1.0, np.abs(want).max()), (t, path, layout)
+    o.close()
+
+
 def test_gmres_iterates_match_oracle(golden):
     """Same CERFACS control flow: same iteration counts, iterates within 1e-10."""
     X, T = golden_layout(golden)
