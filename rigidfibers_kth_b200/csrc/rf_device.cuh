@@ -207,9 +207,12 @@ struct Geom32 {
 };
 
 // FP32 moments for every point of the plain FP32 method and for the far field
-// (c >= near_c >= 10) of the tile mixed-precision kernel.  For c >= 10 the
-// backward recursion alone (moments_backward_fp32; it needs only b and c).
-// Below 10 (plain FP32 method only) the reference's closed forms and forward
+// (c >= near_c >= 10) of the tile mixed-precision kernel.  For c >= 6 the
+// backward recursion alone (moments_backward_fp32; it needs only b and c): the
+// reference switches at 10 in FP64, but its forward recursion amplifies
+// rounding by orders of magnitude as c approaches 10, which FP32 cannot
+// absorb, while from 6 on the backward recursion is accurate to FP32 rounding.
+// Below 6 (plain FP32 method only) the reference's closed forms and forward
 // recursion on ue^2, ub^2 and d formed from the vectors (Geom32), the closed
 // forms rewritten without the cancellation te/ue - tb/ub (which loses all FP32
 // digits when the target point lies near the source axis):
@@ -218,7 +221,7 @@ struct Geom32 {
 template <int N, bool FAR = false>
 __device__ __forceinline__ void moments_fp32(const Geom32 &g, float *I, float *J, float *S) {
     const float b = g.b, c = g.c;
-    if (FAR || c >= 10.0f) {
+    if (FAR || c >= 6.0f) {
         moments_backward_fp32<N>(b, c, I, J, S);
         return;
     }
