@@ -390,6 +390,31 @@ def test_mixed_precision_velocity_error(prec, vmode, layout):
     assert ev <= 1e-6 and ew <= 1e-6, (ev, ew)
 
 
+@pytest.mark.parametrize("N,NoQI", [(1, 8), (2, 4), (3, 8), (4, 6), (6, 8)])
+def test_mixed_precision_other_expansion_orders(N, NoQI):
+    """The split assembly for every expansion order it takes (N = 1..4 here,
+    5 above; its far kernel stages 3N-row column segments whose bulk copies
+    have N-dependent sizes) and the tile kernel's mixed mode beyond it
+    (N = 6): BF16 storage with FP64 refinement, reuse velocities, against the
+    FP64 path on a 200-fiber cloud (a ragged last warp of targets)."""
+    pos, ori = _split_layout("cloud", 200)
+    common = dict(slenderness=1e-3, num_terms_in_force_expansion=N, num_quadrature_intervals=NoQI)
+    with make_sim(pos, ori, gmres_tol=1e-12, gmres_max_iters=1000, **common) as s64:
+        s64.assemble_system()
+        s64.solve_system()
+        s64.update_velocities()
+        V64, W64 = s64.velocities()
+    with make_sim(pos, ori, precision=rf.PREC_MIXED_BF16, gmres_tol=1e-10, gmres_max_iters=300,
+                  velocity_mode=rf.VEL_REUSE, **common) as sim:
+        sim.assemble_system()
+        assert sim.solve_system() == 0
+        sim.update_velocities()
+        V, W = sim.velocities()
+    ev = np.abs(V - V64).max() / np.abs(V64).max()
+    ew = np.abs(W - W64).max() / np.abs(W64).max()
+    assert ev <= 1e-6 and ew <= 1e-6, (N, NoQI, ev, ew)
+
+
 def test_fp32_variant():
     pos, ori = rf.generate_layout(300, "uniform", 5.0, 0.2, seed=1002)
     x64, V64, W64 = _fp64_reference(pos, ori, 1e-3)
