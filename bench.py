@@ -48,6 +48,13 @@ L2_BYTES = 126 * 1024 * 1024
 # the ncu capture summarised in profiles/gemv_bf16_m1000.md; scaled to the
 # workload's matrix size (the traffic grows with the elements streamed)
 TRAFFIC_PER_ELEMENT = (451.270656e6 + 7.171840e6) / (15040 * 15000)
+# Algorithmic work of the assembly: add and multiply flops per ordered fiber
+# pair of the reference formulas (FMA = 2), counted by the oracle's flop
+# counter on this workload's initial layout (6.9 % of the Gauss points in the
+# forward-recursion range); FP32 CUDA-core nominal peak of the B200 (148 SMs x
+# 128 lanes x 2 flops x 1.965 GHz) for the split assembly, whose far field is FP32
+ASM_FLOPS_PER_PAIR = 34916.0
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 # The other configurations of the benchmark (seeded synthetic layouts; half
 # length 1, eps 1e-3, N = 5, 8 x 3 Gauss points, gravity (0,0,-1), minimum
@@ -386,6 +393,15 @@ def run_ours(args):
             "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / world) / plain["value"] if plain else None,
             "velocity_error": verr,
+            "assembly": {"ms": phases["assemble"], "counted_tflop": ASM_FLOPS_PER_PAIR * M * (M - 1) / 1e12,
+                         "achieved_tflops": ASM_FLOPS_PER_PAIR * M * (M - 1) / 1e12 / (phases["assemble"] * 1e-3),
+                         "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_source": "FP32 CUDA-core nominal",
+                         "frac": ASM_FLOPS_PER_PAIR * M * (M - 1) / 1e12 / (phases["assemble"] * 1e-3)
+                         / FP32_NOMINAL_TFLOPS,
+                         "written_gb": (3 * WORKLOAD["N"] * M) * 1.0 * (3 * WORKLOAD["N"] * M) * 6e-9
+                         + 2 * 3 * M * (3 * WORKLOAD["N"] * M) * 4e-9,
+                         "note": "split assembly (classify, near, far, finish) of the phase step; counted work of "
+                                 "the reference formulas at the initial layout"},
         }
     sim.close()
     if world > 1:
