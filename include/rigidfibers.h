@@ -152,6 +152,13 @@ rf_status rf_get_rhs(rf_handle *h, double *b);
 rf_status rf_get_matrix(rf_handle *h, double *A);
 /* y = A x with the stored matrix (FP64 host vectors of n doubles). */
 rf_status rf_matvec(rf_handle *h, const double *x, double *y);
+/* y = A x in FP64 without forming A (mat_prod, fortran/matrix_assembly.f90:159-265):
+ * the identity plus every pair's inner integral against the source's force
+ * expansion from x, projected onto the target's Legendre modes, for the
+ * current state and the handle's inner integral (use_analytical_integration;
+ * the reference's mat_prod uses the numeric one).  Any precision; memory O(M),
+ * work O(M^2) per call.  Host vectors of n doubles. */
+rf_status rf_matvec_free(rf_handle *h, const double *x, double *y);
 rf_status rf_get_solve_stats(rf_handle *h, rf_solve_stats *s);
 /* y = A x in FP64 for callers that cannot allocate device memory: A (n x n
  * column-major, leading dimension lda, lda*n doubles, 16-byte aligned), x and

@@ -120,6 +120,7 @@ def lib():
         "rf_get_rhs": (ctypes.c_int, [_h, _dp]),
         "rf_get_matrix": (ctypes.c_int, [_h, _dp]),
         "rf_matvec": (ctypes.c_int, [_h, _dp, _dp]),
+        "rf_matvec_free": (ctypes.c_int, [_h, _dp, _dp]),
         "rf_get_solve_stats": (ctypes.c_int, [_h, ctypes.POINTER(RfSolveStats)]),
         "rf_matvec_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p]),

@@ -31,7 +31,7 @@ void free_all(rf_handle *h) {
         cudaFree(h->V[i]);
         cudaFree(h->W[i]);
     }
-    void *ptrs[] = {h->tab, h->A64, h->LU, h->lu_r, h->lu_piv, h->lu_info, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
+    void *ptrs[] = {h->tab, h->A64, h->LU, h->lu_r, h->lu_piv, h->lu_info, h->mfpart, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
                     h->PV32, h->PW32, h->vpart, h->pvx, h->pwx, h->work64, h->work32, h->r64, h->r32,
                     h->d32, h->x32, h->Pblocks, h->knn, h->mlp_w, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out,
                     h->dscal, h->rb.partials, h->rb.counter, h->near_bits, h->near_list, h->near_cnt,
@@ -956,6 +956,38 @@ rf_status rf_matvec(rf_handle *h, const double *x, double *y) {
     cudaFree(dx);
     cudaFree(dy);
     CK(h, e, "matvec");
+    return RF_OK;
+}
+
+rf_status rf_matvec_free(rf_handle *h, const double *x, double *y) {
+    if (!h || !x || !y) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    if (!h->mfpart)
+        CK(h, cudaMalloc(&h->mfpart, sizeof(double) * (size_t)h->vel_chunks * h->n), "matrix-free product partials");
+    double *dx = nullptr, *dy = nullptr;
+    CK(h, cudaMalloc(&dx, h->n * 8), "alloc");
+    cudaError_t e = cudaMalloc(&dy, h->n * 8);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, x, h->n * 8, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        rf::MatfreeArgs a{};
+        a.M = h->M;
+        a.N = h->N;
+        a.LQ = h->LQ;
+        a.n = h->n;
+        a.pos = h->X[h->cur];
+        a.ori = h->T[h->cur];
+        a.x = dx;
+        a.tab = h->tab;
+        a.part = h->mfpart;
+        a.chunk = h->vel_chunk;
+        e = rf::launch_matfree(a, h->p.use_analytical_integration == 0, h->vel_chunks, dx, dy, h->stream);
+        h->launches += 2;
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(y, dy, h->n * 8, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dx);
+    cudaFree(dy);
+    CK(h, e, "matrix-free product");
     return RF_OK;
 }
 

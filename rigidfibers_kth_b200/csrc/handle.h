@@ -49,6 +49,7 @@ struct rf_handle {
     int asm_chunks = 1, asm_chunk = 1;
     int vel_chunks = 1, vel_chunk = 1;
     double *velpart = nullptr; // [vel_chunks][6M]
+    double *mfpart = nullptr;  // [vel_chunks][n] matrix-free product partials, made at its first use
     // velocity panels (reuse mode)
     double *PV64 = nullptr, *PW64 = nullptr;
     float *PV32 = nullptr, *PW32 = nullptr;

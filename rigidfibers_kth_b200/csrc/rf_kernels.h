@@ -87,6 +87,19 @@ struct VelArgs {
     int chunk;
 };
 cudaError_t launch_velocity(const VelArgs &a, bool numeric, int nchunks, cudaStream_t st);
+
+// Matrix-free FP64 product y = A x (matfree.cu), the reference's mat_prod.
+struct MatfreeArgs {
+    int M, N, LQ;
+    int64_t n;                 // 3 N M
+    const double *pos, *ori;
+    const double *x;           // n
+    const Tables *tab;
+    double *part;              // [nchunks][n] off-diagonal contributions per source chunk
+    int chunk;
+};
+cudaError_t launch_matfree(const MatfreeArgs &a, bool numeric, int nchunks, const double *x, double *y,
+                           cudaStream_t st);
 // V = (local + 0.5*sum IF0)/d, W = 1.5/d (sum IF1 - (t.sum IF1) t)
 cudaError_t launch_velocity_finish(int M, const double *ori, const Tables *tab, const double *part,
                                    int nchunks, double *V, double *W, cudaStream_t st);

@@ -237,6 +237,13 @@ class Simulation:
         L.check(L.lib().rf_matvec(self._h, _ptr(x), _ptr(y)), self._h)
         return y
 
+    def matvec_free(self, x):
+        """y = A x without forming A (the reference's mat_prod), FP64."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.n)
+        L.check(L.lib().rf_matvec_free(self._h, _ptr(x), _ptr(y)), self._h)
+        return y
+
     def solve_stats(self):
         s = L.RfSolveStats()
         L.check(L.lib().rf_get_solve_stats(self._h, ctypes.byref(s)), self._h)

@@ -145,6 +145,28 @@ def test_one_and_two_fibers_every_path(layout, path):
     o.close()
 
 
+@pytest.mark.parametrize("analytic", [1, 0])
+def test_matrix_free_product_matches_assembled_matrix(golden, analytic):
+    """rf_matvec_free (mat_prod: A x without forming A) against the oracle's
+    assembled matrix and against the handle's own stored FP64 matrix, for the
+    analytic and the numeric inner integral; also from a mixed-precision
+    handle, whose product is FP64 all the same."""
+    X, T = golden_layout(golden)
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(1500)
+    with make_sim(X, T, use_analytical_integration=analytic) as sim:
+        sim.assemble_system()
+        y_stored = sim.matvec(x)
+        y_free = sim.matvec_free(x)
+    A_o, _ = rfo.assemble_system(rfo.make_params(100, analytic=bool(analytic)), X, T)
+    y_o = A_o @ x
+    assert_close64(y_free, y_o, "matrix-free vs oracle A x")
+    assert_close64(y_free, y_stored, "matrix-free vs stored A x")
+    with make_sim(X, T, use_analytical_integration=analytic, precision=rf.PREC_MIXED_BF16) as sim:
+        y_mixed = sim.matvec_free(x)  # no assembly needed: the state alone defines A
+    assert_close64(y_mixed, y_o, "matrix-free from a mixed handle")
+
+
 def test_gmres_iterates_match_oracle(golden):
     """Same CERFACS control flow: same iteration counts, iterates within 1e-10."""
     X, T = golden_layout(golden)
