@@ -125,7 +125,8 @@ void rf_params_default(rf_params *p);
 
 /* Simulation(Configuration): allocate device state for p->num_fibers fibers and
  * upload the initial layout.  Orientations are normalised (as the Fortran
- * driver does, advect_fibers.f90:332-340). */
+ * driver does, advect_fibers.f90:332-340).  One fiber or more; a block
+ * preconditioner needs two or more, the direct solver RF_PREC_FP64. */
 rf_status rf_create(const rf_params *p, const double *positions, const double *orientations,
                     rf_handle **out);
 rf_status rf_destroy(rf_handle *h);
