@@ -4,11 +4,14 @@
 // Reference: LAPACK dgesv called by fortran/coeffs_and_vels.f90:62,158,333,514
 // (the *_direct golden runs).  Blocked right-looking factorisation, panel
 // width kLuNb:
-//   lu_panel_kernel  one CTA factors the tall panel A[k:n, k:k+nb]: per column
-//                    the pivot (first row of largest magnitude, as idamax),
-//                    the row swap inside the panel, the scaling by the
-//                    reciprocal pivot and the rank-1 update of the panel's
-//                    remaining columns (dgetf2's steps);
+//   lu_panel_kernel  one CTA factors 8 columns of the tall panel
+//                    A[k:n, k:k+nb]: per column the pivot (first row of
+//                    largest magnitude, as idamax), the row swap across the
+//                    panel, the scaling by the reciprocal pivot and the rank-1
+//                    update of the 8 columns (dgetf2's steps; the last three
+//                    and the next pivot search in one pass over the rows);
+//   lu_panel_update_kernel  the 8 columns' update of the rest of the panel,
+//                    over the whole GPU;
 //   lu_swap_kernel   the panel's row swaps applied to the trailing columns;
 //   lu_trsm_kernel   U12 = L11^-1 A12, one thread per trailing column;
 //   lu_gemm_kernel   A22 -= L21 U12, 64 x 64 tiles staged in shared memory.
@@ -24,7 +27,8 @@ namespace rf {
 namespace {
 
 constexpr int kLuNb = 32;
-constexpr int kPanelThreads = 512;
+constexpr int kLuSub = 8;   // sub-panel width: the columns one CTA factors
+constexpr int kPanelThreads = 1024;
 
 __device__ __forceinline__ void argmax_merge(double &v, int64_t &i, double ov, int64_t oi) {
     if (ov > v || (ov == v && oi < i)) {
@@ -33,34 +37,52 @@ __device__ __forceinline__ void argmax_merge(double &v, int64_t &i, double ov, i
     }
 }
 
-__global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb,
-                                                                int *piv, int *info) {
-    __shared__ double s_val[kPanelThreads / 32];
-    __shared__ int64_t s_idx[kPanelThreads / 32];
-    __shared__ int64_t s_piv;
+// Block-wide first-maximum reduction of (value, row) pairs; every thread gets
+// the result.
+__device__ __forceinline__ int64_t block_argmax(double best, int64_t bi, int64_t none, double *s_val,
+                                                int64_t *s_idx) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    for (int j = 0; j < nb; ++j) {
-        const int64_t col = k + j;
-        double *cj = A + col * lda;
-        double best = -1.0;
-        int64_t bi = n;
-        for (int64_t r = col + tid; r < n; r += blockDim.x) argmax_merge(best, bi, fabs(cj[r]), r);
+    for (int o = 16; o; o >>= 1)
+        argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, o), __shfl_down_sync(0xffffffffu, bi, o));
+    if (lane == 0) {
+        s_val[warp] = best;
+        s_idx[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        best = lane < nwarps ? s_val[lane] : -1.0;
+        bi = lane < nwarps ? s_idx[lane] : none;
         for (int o = 16; o; o >>= 1)
             argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, o), __shfl_down_sync(0xffffffffu, bi, o));
-        if (lane == 0) {
-            s_val[warp] = best;
-            s_idx[warp] = bi;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            best = lane < nwarps ? s_val[lane] : -1.0;
-            bi = lane < nwarps ? s_idx[lane] : n;
-            for (int o = 16; o; o >>= 1)
-                argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, o), __shfl_down_sync(0xffffffffu, bi, o));
-            if (lane == 0) s_piv = bi < n ? bi : col;  // a column of NaN keeps its row
-        }
-        __syncthreads();
-        const int64_t p = s_piv;
+        if (lane == 0) s_idx[0] = bi;
+    }
+    __syncthreads();
+    const int64_t r = s_idx[0];
+    __syncthreads();  // s_idx is reused by the next reduction
+    return r;
+}
+
+// Sub-panel factorisation: columns [s0, s0 + sb) of the panel [k, k + nb),
+// one CTA.  One pass per column over the rows below the diagonal: scale the
+// column by the reciprocal pivot, update the sub-panel's remaining columns
+// (the pivot row's entries staged in shared memory) and, in the same pass,
+// find the next column's pivot among the updated values.  Row swaps cover
+// all nb columns of the panel, so its L is consistent.  Then U of the
+// sub-panel's rows for the panel's columns right of it (unit lower sb x sb
+// triangle, one thread per column).
+__global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb,
+                                                                int64_t s0, int sb, int *piv, int *info) {
+    __shared__ double s_val[kPanelThreads / 32];
+    __shared__ int64_t s_idx[kPanelThreads / 32];
+    __shared__ double s_u[kLuSub];
+    const int tid = threadIdx.x;
+    double best = -1.0;
+    int64_t bi = n;
+    for (int64_t r = s0 + tid; r < n; r += blockDim.x) argmax_merge(best, bi, fabs(A[s0 * lda + r]), r);
+    int64_t p = block_argmax(best, bi, n, s_val, s_idx);
+    for (int j = 0; j < sb; ++j) {
+        const int64_t col = s0 + j;
+        if (p >= n) p = col;  // a column of NaN keeps its row
         if (tid == 0) piv[col] = (int)p;
         if (p != col && tid < nb) {
             double *c = A + (k + tid) * lda;
@@ -69,21 +91,63 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int6
             c[p] = t;
         }
         __syncthreads();
+        double *cj = A + col * lda;
         const double d = cj[col];
-        if (d == 0.0) {
-            if (tid == 0 && *info == 0) *info = (int)(col + 1);
-        } else {
-            const double inv = 1.0 / d;
-            for (int64_t r = col + 1 + tid; r < n; r += blockDim.x) cj[r] *= inv;
-        }
+        if (tid < sb) s_u[tid] = tid > j ? A[(s0 + tid) * lda + col] : 0.0;
+        if (d == 0.0 && tid == 0 && *info == 0) *info = (int)(col + 1);
         __syncthreads();
-        for (int c = j + 1; c < nb; ++c) {
-            double *cc = A + (k + c) * lda;
-            const double u = cc[col];
-            if (u != 0.0)
-                for (int64_t r = col + 1 + tid; r < n; r += blockDim.x) cc[r] = fma(-cj[r], u, cc[r]);
+        const double inv = d != 0.0 ? 1.0 / d : 0.0;  // a zero pivot leaves a zero column (dgetf2)
+        best = -1.0;
+        bi = n;
+        for (int64_t r = col + 1 + tid; r < n; r += blockDim.x) {
+            const double x = d != 0.0 ? cj[r] * inv : cj[r];
+            cj[r] = x;
+            for (int c = j + 1; c < sb; ++c) {
+                double *cc = A + (s0 + c) * lda;
+                const double v = fma(-x, s_u[c], cc[r]);
+                cc[r] = v;
+                if (c == j + 1) argmax_merge(best, bi, fabs(v), r);
+            }
         }
-        __syncthreads();
+        if (j + 1 < sb) p = block_argmax(best, bi, n, s_val, s_idx);
+        else __syncthreads();
+    }
+    // U rows of the sub-panel for the panel's columns right of it
+    const int64_t c = s0 + sb + tid;
+    if (c < k + nb && c < n) {
+        double *col = A + c * lda + s0;
+        for (int i = 1; i < sb; ++i) {
+            double v = col[i];
+            for (int q = 0; q < i; ++q) v = fma(-A[(s0 + q) * lda + s0 + i], col[q], v);
+            col[i] = v;
+        }
+    }
+}
+
+// The sub-panel's rank-sb update of the panel's columns right of it:
+// A[r, c] -= sum_q A[r, s0 + q] A[s0 + q, c] for rows r >= s0 + sb and columns
+// c in [s0 + sb, k + nb); one thread per row, the U entries in shared memory.
+__global__ void __launch_bounds__(256) lu_panel_update_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb,
+                                                             int64_t s0, int sb) {
+    __shared__ double s_uu[kLuNb][kLuSub];
+    const int64_t c0 = s0 + sb, c1 = std::min<int64_t>(k + nb, n);
+    const int nc = (int)(c1 - c0);
+    for (int t = threadIdx.x; t < nc * sb; t += blockDim.x) {
+        const int c = t / sb, q = t % sb;
+        s_uu[c][q] = A[(c0 + c) * lda + s0 + q];
+    }
+    __syncthreads();
+    const int64_t r = s0 + sb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    double l[kLuSub];
+#pragma unroll
+    for (int q = 0; q < kLuSub; ++q) l[q] = q < sb ? A[(s0 + q) * lda + r] : 0.0;
+    for (int c = 0; c < nc; ++c) {
+        double v = A[(c0 + c) * lda + r];
+#pragma unroll
+        for (int q = 0; q < kLuSub; ++q)
+            if (q < sb) v = fma(-l[q], s_uu[c][q], v);
+        A[(c0 + c) * lda + r] = v;
     }
 }
 
@@ -218,8 +282,16 @@ cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, cu
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), st);
     for (int64_t k = 0; k < n && e == cudaSuccess; k += kLuNb) {
         const int nb = (int)std::min<int64_t>(kLuNb, n - k);
-        lu_panel_kernel<<<1, kPanelThreads, 0, st>>>(A, lda, n, k, nb, piv, info);
-        ++*launches;
+        for (int s0 = 0; s0 < nb; s0 += kLuSub) {
+            const int sb = std::min(kLuSub, nb - s0);
+            lu_panel_kernel<<<1, kPanelThreads, 0, st>>>(A, lda, n, k, nb, k + s0, sb, piv, info);
+            ++*launches;
+            if (s0 + sb < nb && k + s0 + sb < n) {
+                lu_panel_update_kernel<<<(unsigned)cdiv(n - k - s0 - sb, 256), 256, 0, st>>>(A, lda, n, k, nb, k + s0,
+                                                                                          sb);
+                ++*launches;
+            }
+        }
         const int64_t rest = n - k - nb;
         if (rest > 0) {
             lu_swap_kernel<<<(unsigned)cdiv(rest, 128), 128, 0, st>>>(A, lda, n, k, nb, k + nb, piv);
