@@ -286,9 +286,8 @@ template <int N, bool PANELS>
 struct FarSmem {
     static constexpr int GR = 32 * 3 * N;                   // staged rows of one column
     static constexpr int PAN = 2 * 3 * 96;                  // staged panel columns
-    static constexpr int SET = (N + 1) * 7 * 32;            // coefficient sets of one weight [k][7][lane]
     static constexpr int STG16 = 3 * GR / 2;                // BF16 copy of the staged columns (in floats)
-    static constexpr size_t kBytes = sizeof(float) * (32 * kNearWeight + SET + 16 + 64 + kMaxLQ +
+    static constexpr size_t kBytes = sizeof(float) * (32 * kNearWeight + 16 + 64 + kMaxLQ +
                                                       kMaxLQ * SplitDims<N>::KW + 3 * GR + (PANELS ? PAN : 0) +
                                                       STG16);
     static_assert(kBytes % 16 == 0, "each warp's region starts on a 16-byte boundary");
@@ -378,12 +377,12 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
     }
 }
 
-// Coefficient sets of weight m (parity PAR) for rows k = 0..N, staged per
-// lane as [k][AI, R0, R1, R2, C0, C1, E][lane].
+// Coefficient sets of weight m (parity PAR) for rows k = 0..N in registers:
+// S[0..6][k] = AI, R0, R1, R2, C0, C1, E.
 template <int N, int PAR>
-__device__ __forceinline__ void far_sets(int m, const float (&U)[N + 1][N + 1], const float (&V)[N + 3][N + 3],
-                                         float *s_set, int lane) {
-    constexpr int NP = (N - PAR) / 2 + 1;  // p = PAR, PAR + 2, ... <= N
+__device__ __forceinline__ void far_sets_reg(int m, const float (&U)[N + 1][N + 1], const float (&V)[N + 3][N + 3],
+                                             float (&S)[7][N + 1]) {
+    constexpr int NP = (N - PAR) / 2 + 1;
     float cf[NP];
 #pragma unroll
     for (int i = 0; i < NP; ++i) cf[i] = c_leg32[m][PAR + 2 * i];
@@ -414,21 +413,21 @@ __device__ __forceinline__ void far_sets(int m, const float (&U)[N + 1][N + 1], 
             ai = fmaf(cf[i], U[PAR + 2 * i][k], ai);
             ee = fmaf(cf[i], V[PAR + 2 * i + 2][k], ee);
         }
-        float *o = s_set + k * 7 * 32 + lane;
-        o[0] = ai;
-        o[32] = R0[k];
-        o[64] = R1[k];
-        o[96] = (float)bonnet_a(k) * R1[k + 1] + (k > 0 ? (float)bonnet_b(k) * R1[k > 0 ? k - 1 : 0] : 0.f);
-        o[128] = C0[k];
-        o[160] = (float)bonnet_a(k) * C0[k + 1] + (k > 0 ? (float)bonnet_b(k) * C0[k > 0 ? k - 1 : 0] : 0.f);
-        o[192] = ee;
+        S[0][k] = ai;
+        S[1][k] = R0[k];
+        S[2][k] = R1[k];
+        S[3][k] = (float)bonnet_a(k) * R1[k + 1] + (k > 0 ? (float)bonnet_b(k) * R1[k > 0 ? k - 1 : 0] : 0.f);
+        S[4][k] = C0[k];
+        S[5][k] = (float)bonnet_a(k) * C0[k + 1] + (k > 0 ? (float)bonnet_b(k) * C0[k > 0 ? k - 1 : 0] : 0.f);
+        S[6][k] = ee;
     }
 }
 
-// X = R0 D + R1 t + C0 p, Y = R1 D + R2 t + C1 p, Z = C0 D + C1 t + E p
-__device__ __forceinline__ void far_xyz(const float *o, const float *D, const float *t, const float *p, float *X,
-                                        float *Y, float *Z) {
-    const float R0 = o[32], R1 = o[64], R2 = o[96], C0 = o[128], C1 = o[160], E = o[192];
+// X = R0 D + R1 t + C0 p, Y = R1 D + R2 t + C1 p, Z = C0 D + C1 t + E p for row k
+template <int N>
+__device__ __forceinline__ void far_xyz_r(const float (&S)[7][N + 1], int k, const float *D, const float *t,
+                                          const float *p, float *X, float *Y, float *Z) {
+    const float R0 = S[1][k], R1 = S[2][k], R2 = S[3][k], C0 = S[4][k], C1 = S[5][k], E = S[6][k];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         X[c] = R0 * D[c] + R1 * t[c] + C0 * p[c];
@@ -436,6 +435,7 @@ __device__ __forceinline__ void far_xyz(const float *o, const float *D, const fl
         Z[c] = C0 * D[c] + C1 * t[c] + E * p[c];
     }
 }
+
 
 template <int N, bool PANELS, bool FAR>
 __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS) far_pairs_kernel(SplitArgs a) {
@@ -446,8 +446,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned char *smem_raw = smem_all + (size_t)warp * SM::kBytes;  // this warp's region
     float *s_nb = reinterpret_cast<float *>(smem_raw);               // [near lane][kNearWeight], one weight
-    float *s_set = s_nb + 32 * kNearWeight;                           // [k][7][32]
-    float *s_gk = s_set + SM::SET;                                    // gamma_k (0..7), E_k (8..15)
+    float *s_gk = s_nb + 32 * kNearWeight;                            // gamma_k (0..7), E_k (8..15)
     int *s_nl = reinterpret_cast<int *>(s_gk + 16);                   // near lanes of the source, in order
     int *s_ns = s_nl + 32;                                            // and their buffer slots
     float *s_pv = reinterpret_cast<float *>(s_ns + 32);
@@ -624,14 +623,14 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
             // the copy engine has read the previous weight's staged columns
             if (lane == 0) bulk_wait_read();
             __syncwarp();
-            if (m & 1) far_sets<N, 1>(m, U, V, s_set, lane);
-            else far_sets<N, 0>(m, U, V, s_set, lane);
-            const float *o = s_set + lane;
+            float S[7][N + 1];
+            if (m & 1) far_sets_reg<N, 1>(m, U, V, S);
+            else far_sets_reg<N, 0>(m, U, V, S);
             // row k = 0: velocity panel P0 only
             if (PANELS) {
                 float X[3], Y[3], Z[3];
-                far_xyz(o, D, t, p, X, Y, Z);
-                const float AI = o[0];
+                far_xyz_r<N>(S, 0, D, t, p, X, Y, Z);
+                const float AI = S[0][0];
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
@@ -641,10 +640,9 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
             }
             // row k = 1: block row D1 t (theta t)^T and velocity panel P1
             {
-                const float *o1 = o + 7 * 32;
                 float X[3], Y[3], Z[3], Q[3];
-                far_xyz(o1, D, t, p, X, Y, Z);
-                const float AI = o1[0];
+                far_xyz_r<N>(S, 1, D, t, p, X, Y, Z);
+                const float AI = S[0][1];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) Q[c] = AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c];
 #pragma unroll
@@ -661,12 +659,11 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
                 }
             }
             // rows k = 2..N: gamma_k (theta - E_k t (theta t)^T)
-#pragma unroll 1
+#pragma unroll
             for (int k = 2; k <= N; ++k) {
-                const float *ok = o + k * 7 * 32;
                 float X[3], Y[3], Z[3], W[3];
-                far_xyz(ok, D, t, p, X, Y, Z);
-                const float AI = ok[0], g = s_gk[k], ek = s_gk[8 + k];
+                far_xyz_r<N>(S, k, D, t, p, X, Y, Z);
+                const float AI = S[0][k], g = s_gk[k], ek = s_gk[8 + k];
 #pragma unroll
                 for (int c = 0; c < 3; ++c) W[c] = Y[c] - ek * (AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c]);
                 float *dst = s_stg + lane * RB + 3 * (k - 1);
