@@ -324,19 +324,6 @@ __device__ __forceinline__ void g_tensor(const T *I, const T *J, const T *S, con
     for (int c = 0; c < 6; ++c) G[c] = cRR * o.rr[c] + cPR * o.pr[c] + cPP * o.pp[c] + (c < 3 ? cI : (T)0);
 }
 
-template <typename T, int N, int m = 0>
-struct GAll {
-    __device__ __forceinline__ static void run(const T *I, const T *J, const T *S, const Outer<T> &o, T eps2,
-                                               T (*G)[6]) {
-        g_tensor<T, m>(I, J, S, o, eps2, G[m]);
-        GAll<T, N, m + 1>::run(I, J, S, o, eps2, G);
-    }
-};
-template <typename T, int N>
-struct GAll<T, N, N + 1> {
-    __device__ __forceinline__ static void run(const T *, const T *, const T *, const Outer<T> &, T, T (*)[6]) {}
-};
-
 // Store G_m for m = 0..N straight to shared memory as it is formed:
 // dst[(m*6 + c) * ld], converting to double.
 template <typename T, int N, int m = 0>
@@ -379,21 +366,6 @@ struct GForce<T, N, N + 1> {
                                                const T (*)[3], T *) {}
 };
 
-// Analytic inner integral over the source fiber (centre xb, direction pb) at
-// target point xbar, for all Legendre weights m = 0..N:
-// G[m][c] = int_{-1}^{1} K(xbar - xb - s pb) P_m(s) ds  (FP64, reference formulas).
-template <int N>
-__device__ __forceinline__ void inner_analytic_fp64(double r0x, double r0y, double r0z, double px, double py,
-                                                    double pz, double eps2, double (*G)[6]) {
-    double I[N + 3], J[N + 3], S[N + 3];
-    // b = -2 SUM(pb*R0), c = SUM(R0**2)  (Int_analytical.f90:83-87)
-    const double b = fmul(-2.0, fadd(fadd(fmul(px, r0x), fmul(py, r0y)), fmul(pz, r0z)));
-    const double c = fadd(fadd(fmul(r0x, r0x), fmul(r0y, r0y)), fmul(r0z, r0z));
-    moments_fp64<N>(b, c, I, J, S);
-    const Outer<double> o(r0x, r0y, r0z, px, py, pz);
-    GAll<double, N>::run(I, J, S, o, eps2, G);
-}
-
 // The analytic inner integral for all weights, stored to shared memory.
 template <int N>
 __device__ __forceinline__ void inner_analytic_store_fp64(double r0x, double r0y, double r0z, double px, double py,
@@ -425,15 +397,6 @@ __device__ __forceinline__ void inner_analytic_force_fp64(double r0x, double r0y
     const double c = fadd(fadd(fmul(r0x, r0x), fmul(r0y, r0y)), fmul(r0z, r0z));
     moments_fp64<N>(b, c, I, J, S);
     GForce<double, N>::run(I, J, S, r0x, r0y, r0z, px, py, pz, eps2, f, u);
-}
-
-template <int N>
-__device__ __forceinline__ void inner_analytic_fp32(float r0x, float r0y, float r0z, float px, float py,
-                                                    float pz, float eps2, float (*G)[6]) {
-    float I[N + 3], J[N + 3], S[N + 3];
-    moments_fp32<N>(Geom32(r0x, r0y, r0z, px, py, pz), I, J, S);
-    const Outer<float> o(r0x, r0y, r0z, px, py, pz);
-    GAll<float, N>::run(I, J, S, o, eps2, G);
 }
 
 // Numeric inner integral (quadrature.f90:100-164): 3-point Gauss on each
