@@ -93,3 +93,32 @@ def test_reference_closed_forms_cancel_for_distant_pairs_in_fp32():
     assert abs(i1 - I[1]) / abs(I[1]) > 1e-2
     got = backward_fp32(b, c)[0]
     assert abs(got[1] - I[1]) / abs(I[1]) <= 1e-5
+
+
+def test_fp32_geometry_of_touching_fibers_from_the_vectors():
+    """A target point 5e-5 from a source fiber's line (fibers that cross,
+    as in the uniform layouts): d = c - b^2/4 formed from b and c rounds to
+    zero or below in FP32, while |R0 x p|^2 keeps its relative accuracy; the
+    same holds for ue^2 = |R0 - p|^2 near the fiber's end (Geom32)."""
+    p = np.array([0.6, 0.0, 0.8])
+    n = np.array([0.8, 0.0, -0.6])  # unit, perpendicular to p
+    for s0, delta in ((0.3, 5e-5), (-0.7, 2e-5), (0.999, 3e-5)):
+        R0 = s0 * p + delta * n
+        d_true = delta * delta
+        r = R0.astype(np.float32)
+        pf = p.astype(np.float32)
+        b = f32(-2) * f32(np.dot(pf, r))
+        c = f32(np.dot(r, r))
+        d_from_bc = float(c - f32(0.25) * b * b)
+        cr = np.cross(r, pf).astype(np.float32)
+        d_vec = float(np.dot(cr, cr))
+        assert abs(d_vec - d_true) / d_true < 1e-3
+        assert abs(d_from_bc - d_true) / d_true > 1e-2  # cancellation: no digit left
+    # ue^2 = 1 + b + c at a point 3e-5 beyond the source's end
+    R0 = (1.0 + 3e-5) * p
+    r = R0.astype(np.float32)
+    ue2_vec = float(np.dot(r - pf, r - pf))
+    b = f32(-2) * f32(np.dot(pf, r))
+    ue2_bc = float(f32(1) + b + f32(np.dot(r, r)))
+    assert abs(ue2_vec - 9e-10) / 9e-10 < 1e-2
+    assert abs(ue2_bc - 9e-10) / 9e-10 > 1e-1
