@@ -65,3 +65,23 @@ def test_two_gloo_ranks_barrier_and_max_over_ranks():
         assert d["world"] == 2 and d["backend"] == "gloo"
         assert d["max"] == 2.5  # the slowest rank's time is the job's time
     assert outs[1]["ref"] is None  # the reference arm runs on rank 0 only
+
+
+def test_reference_arm_json_line_contract():
+    """`bench.py --impl reference` on one process (a small M keeps it short):
+    one JSON line with the contract's keys, the CPU baseline describing the
+    run and an end-to-end figure without host-device traffic."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--M", "40",
+                        "--steps", "1", "--warmup", "0"], cwd=ROOT, env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
