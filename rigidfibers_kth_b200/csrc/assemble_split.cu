@@ -13,11 +13,13 @@
 // to the source axis).  Three kernels:
 //   classify_kernel   one warp per target: near-pair bitmap and per-target
 //                     lists in ascending source order;
-//   far_pairs_kernel  FP32, lane = target fiber, warp-uniform source: every
-//                     lane integrates its own pair over the target's Gauss
-//                     points with the projection accumulated in registers,
-//                     then stages the 3N x 3N block in shared memory and the
-//                     warp writes whole column segments;
+//   far_pairs_kernel  FP32, lane = target fiber, warp-uniform source, eight
+//                     warps per CTA stepping through the sources together:
+//                     every lane integrates its own pair over the target's
+//                     Gauss points with the projection accumulated in
+//                     registers, then stages the 3N x 3N block (and its BF16
+//                     copy and the velocity-panel rows) in shared memory and
+//                     one lane hands whole column segments to the copy engine;
 //   near_pairs_kernel FP64, one warp per near pair: lane = Gauss point, the
 //                     projection on the FP64 tensor cores (mma.sync m8n8k4).
 // A finish kernel sums the per-chunk right-hand-side partials in a fixed order.
