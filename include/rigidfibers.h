@@ -151,6 +151,13 @@ rf_status rf_get_coeffs(rf_handle *h, double *x);
 rf_status rf_get_rhs(rf_handle *h, double *b);
 /* Dense matrix, n*n doubles column-major (converted from the stored precision). */
 rf_status rf_get_matrix(rf_handle *h, double *A);
+/* Rows [row0, row0 + rows) of the stored matrix as FP64, rows x n
+ * column-major (leading dimension rows), for checking a sample of a system
+ * too large to copy whole (the reference dumps all of A,
+ * src/simulation.cu:468-546).  which = 0: the matrix of the FP64 path or of
+ * the refinement residual (FP64 or FP32 storage); which = 1: the matrix of
+ * the inner solve (the BF16 copy where there is one, else as 0). */
+rf_status rf_get_matrix_rows(rf_handle *h, int32_t which, int64_t row0, int64_t rows, double *out);
 /* y = A x with the stored matrix (FP64 host vectors of n doubles). */
 rf_status rf_matvec(rf_handle *h, const double *x, double *y);
 /* y = A x in FP64 without forming A (mat_prod, fortran/matrix_assembly.f90:159-265):
@@ -163,18 +170,21 @@ rf_status rf_matvec_free(rf_handle *h, const double *x, double *y);
 rf_status rf_get_solve_stats(rf_handle *h, rf_solve_stats *s);
 /* y = A x in FP64 for callers that cannot allocate device memory: A (n x n
  * column-major, leading dimension lda, lda*n doubles, 16-byte aligned), x and
- * y are the caller's device buffers, and the product's partial sums use an
- * 8 MiB array that the library reserves on every GPU that loads it, kept
- * until the process exits.  No counterpart in the reference: it serves hosts
- * whose device memory belongs to their own allocator or pool, and loops that
- * must not stall on cudaMalloc/cudaFree.  Limit: lda <= 1,048,576 (lda even);
- * larger sizes return RF_ERR_INVALID_ARG with the reason in
- * rf_last_error(NULL).  Enqueued on `stream` (cudaStream_t, NULL = default
- * stream) of the current device; y is ready when the stream reaches it.  The
- * first call on a device looks up the array's device address, so make that
- * call before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (other streams, other threads) race on it.  Nothing in
- * the array needs to start at zero. */
+ * y are the caller's device buffers, and the product's partial sums use a
+ * fixed 8 MiB array inside the library.  No counterpart in the reference: it
+ * serves hosts whose device memory belongs to their own allocator or pool,
+ * and loops that must not stall on cudaMalloc/cudaFree.  Limit: lda <=
+ * 1,048,576 (lda even); larger sizes return RF_ERR_INVALID_ARG with the
+ * reason in rf_last_error(NULL).  Enqueued on `stream` (cudaStream_t, NULL =
+ * default stream) of the current device; y is ready when the stream reaches
+ * it.  The first call on a device sets the array up: it looks up the array's
+ * device address, and with CUDA's default lazy module loading that is also
+ * when the driver loads the library's device code and reserves the 8 MiB on
+ * that device (it may synchronise the device); the array then stays until the
+ * process exits.  So make the first call on each device before a memory pool
+ * claims the device's memory and before any stream capture.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other threads)
+ * race on it.  Nothing in the array needs to start at zero. */
 rf_status rf_matvec_noalloc(const double *A, int64_t lda, int64_t n, const double *x, double *y, void *stream);
 /* Multistep history for checkpoint/resume: previous positions/orientations
  * and previous velocities (3*M doubles each). */

@@ -12,10 +12,14 @@
 #include "rfo.h"
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
+#include <map>
+#include <memory>
 #include <vector>
 
 #ifdef _OPENMP
@@ -405,6 +409,69 @@ double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Random stream of the synthetic layouts: xoshiro256** (Blackman and Vigna)
+// whose four state words come from splitmix64 of the seed.  Uniform variates
+// take the top 53 bits; normal variates are one Box-Muller value per call.
+struct LayoutRng {
+    uint64_t w[4];
+    explicit LayoutRng(uint64_t seed) {
+        uint64_t z = seed;
+        for (uint64_t &s : w) {
+            z += 0x9e3779b97f4a7c15ull;
+            uint64_t v = z;
+            v = (v ^ (v >> 30)) * 0xbf58476d1ce4e5b9ull;
+            v = (v ^ (v >> 27)) * 0x94d049bb133111ebull;
+            s = v ^ (v >> 31);
+        }
+    }
+    static uint64_t rotl(uint64_t v, int k) { return (v << k) | (v >> (64 - k)); }
+    uint64_t bits() {
+        const uint64_t out = rotl(w[1] * 5, 7) * 9;
+        const uint64_t sh = w[1] << 17;
+        w[2] ^= w[0];
+        w[3] ^= w[1];
+        w[1] ^= w[2];
+        w[0] ^= w[3];
+        w[2] ^= sh;
+        w[3] = rotl(w[3], 45);
+        return out;
+    }
+    double u01() { return (double)(bits() >> 11) * (1.0 / 9007199254740992.0); }
+    double gauss() {
+        double a = u01();
+        while (a <= 0.0) a = u01();
+        const double b = u01();
+        return std::sqrt(-2.0 * std::log(a)) * std::cos(2.0 * M_PI * b);
+    }
+};
+
+int assemble_rows_ld(const rfo_params *p, const double *X, const double *T, int i0, int i1, double *Arows,
+                     size_t ld, double *brows) {
+    // rows of target fibers [i0, i1): Arows[r + col * ld], r = (i - i0) * 3N + row in the block
+    if (!p || p->N < 1 || p->N > kMaxN || p->M < 1 || p->NoQI < 1 || 3 * p->NoQI > kMaxLQ) return -1;
+    set_threads(p->threads);
+    const Tables t = make_tables(p->N, p->NoQI);
+    const Consts k = make_consts(p->eps, p->N);
+    const int M = p->M, n3 = 3 * p->N;
+#pragma omp parallel
+    {
+        std::vector<double> blk((size_t)M * n3 * n3);
+#pragma omp for schedule(dynamic, 1)
+        for (int i = i0; i < i1; ++i) {
+            double *brow = brows + (size_t)(i - i0) * n3;
+            assemble_target(p, t, k, X, T, i, blk.data(), brow);
+            for (int j = 0; j < M; ++j)
+                for (int cl = 0; cl < n3; ++cl) {
+                    const size_t col = (size_t)j * n3 + cl;
+                    double *dst = Arows + col * ld + (size_t)(i - i0) * n3;
+                    const double *src = &blk[((size_t)j * n3 + cl) * n3];
+                    for (int r = 0; r < n3; ++r) dst[r] = src[r];
+                }
+        }
+    }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -462,31 +529,7 @@ void rfo_analytic_moments(const double *xb, const double *pb, const double *xbar
 
 int rfo_assemble_rows(const rfo_params *p, const double *X, const double *T, int i0, int i1,
                       double *Arows, double *brows) {
-    if (!p || p->N < 1 || p->N > kMaxN || p->M < 1 || p->NoQI < 1 || 3 * p->NoQI > kMaxLQ) return -1;
-    set_threads(p->threads);
-    const Tables t = make_tables(p->N, p->NoQI);
-    const Consts k = make_consts(p->eps, p->N);
-    const int M = p->M, n3 = 3 * p->N;
-    const size_t n = (size_t)n3 * M;
-    const size_t ld = (size_t)(i1 - i0) * n3;
-#pragma omp parallel
-    {
-        std::vector<double> blk((size_t)M * n3 * n3);
-#pragma omp for schedule(dynamic, 1)
-        for (int i = i0; i < i1; ++i) {
-            double *brow = brows + (size_t)(i - i0) * n3;
-            assemble_target(p, t, k, X, T, i, blk.data(), brow);
-            for (int j = 0; j < M; ++j)
-                for (int cl = 0; cl < n3; ++cl) {
-                    const size_t col = (size_t)j * n3 + cl;
-                    double *dst = Arows + col * ld + (size_t)(i - i0) * n3;
-                    const double *src = &blk[((size_t)j * n3 + cl) * n3];
-                    for (int r = 0; r < n3; ++r) dst[r] = src[r];
-                }
-        }
-    }
-    (void)n;
-    return 0;
+    return assemble_rows_ld(p, X, T, i0, i1, Arows, (size_t)(i1 - i0) * 3 * (p ? p->N : 0), brows);
 }
 
 int rfo_assemble_system(const rfo_params *p, const double *X, const double *T, double *A, double *b) {
@@ -709,6 +752,10 @@ struct rfo_sim {
     std::vector<double> X[3], T[3], V[2], W[2];
     int prev = 0, cur = 1, next = 2, vold = 0, vnew = 1;
     std::vector<double> init_guess, coeffs, b;
+    // the step's system matrix (n x n column-major), allocated at the first
+    // assembly and kept for the following steps; every entry is rewritten
+    std::unique_ptr<double[]> A;
+    double assemble_s = 0.0;
     int info = 0, iters = 0;
     double be = 0.0;
     double t4[4] = {0, 0, 0, 0};
@@ -736,28 +783,45 @@ rfo_sim *rfo_sim_create(const rfo_params *p, const double *X0, const double *T0)
 
 void rfo_sim_destroy(rfo_sim *s) { delete s; }
 
-int rfo_sim_step(rfo_sim *s) {
+int rfo_sim_assemble_part(rfo_sim *s, int i0, int i1) {
+    // Rows of the step's A and b that belong to target fibers [i0, i1)
+    // (matrix_assembly.f90:407-629, 796-905 restricted to those targets).
+    const rfo_params &p = s->p;
+    if (i0 < 0 || i1 > p.M || i0 > i1) return -1;
+    const size_t n = 3 * (size_t)p.M * p.N;
+    if (!s->A) s->A.reset(new double[n * n]);
+    if (i0 == i1) return 0;
+    const double t0 = now_s();
+    const size_t r0 = (size_t)i0 * 3 * p.N;
+    const int rc = assemble_rows_ld(&p, s->X[s->cur].data(), s->T[s->cur].data(), i0, i1, s->A.get() + r0,
+                                    n, s->b.data() + r0);
+    s->assemble_s += now_s() - t0;
+    return rc;
+}
+
+int rfo_sim_finish_step(rfo_sim *s) {
+    // The rest of the time step on the assembled system: solve, velocities,
+    // advection, rotation of the state buffers (advect_fibers.f90:437-593).
     const rfo_params &p = s->p;
     const int M = p.M;
     const size_t m3 = 3 * (size_t)M, n = m3 * p.N;
-    std::vector<double> A(n * n);
-    double t0 = now_s();
+    if (!s->A) return -1;
+    double *A = s->A.get();
     const double *X = s->X[s->cur].data(), *T = s->T[s->cur].data();
-    rfo_assemble_system(&p, X, T, A.data(), s->b.data());
     double t1 = now_s();
     // solve (coeffs_and_vels.f90:80-172 direct, 361-532 GMRES with LU fallback)
     if (p.direct) {
         s->coeffs = s->b;
-        s->info = rfo_solve_direct((int)n, A.data(), s->coeffs.data());
+        s->info = rfo_solve_direct((int)n, A, s->coeffs.data());
         s->iters = 0;
         s->be = 0.0;
     } else {
         s->coeffs = s->init_guess;
-        s->info = rfo_solve_gmres((int)n, A.data(), s->b.data(), s->coeffs.data(), p.restart, p.max_iters,
+        s->info = rfo_solve_gmres((int)n, A, s->b.data(), s->coeffs.data(), p.restart, p.max_iters,
                                   p.tol, &s->iters, &s->be, p.threads);
         if (s->info == -4) {
             s->coeffs = s->b;
-            rfo_solve_direct((int)n, A.data(), s->coeffs.data());
+            rfo_solve_direct((int)n, A, s->coeffs.data());
         }
     }
     s->init_guess = s->coeffs;
@@ -794,8 +858,15 @@ int rfo_sim_step(rfo_sim *s) {
     s->cur = s->next;
     s->next = oldprev;
     s->step++;
-    s->t4[0] = t1 - t0; s->t4[1] = t2 - t1; s->t4[2] = t3 - t2; s->t4[3] = t4 - t3;
+    s->t4[0] = s->assemble_s; s->t4[1] = t2 - t1; s->t4[2] = t3 - t2; s->t4[3] = t4 - t3;
+    s->assemble_s = 0.0;
     return s->info == -4 ? 1 : 0;
+}
+
+int rfo_sim_step(rfo_sim *s) {
+    const int rc = rfo_sim_assemble_part(s, 0, s->p.M);
+    if (rc != 0) return rc;
+    return rfo_sim_finish_step(s);
 }
 
 void rfo_sim_last(const rfo_sim *s, double *b, double *coeffs, double *V, double *W, double *X, double *T) {
@@ -816,6 +887,69 @@ void rfo_sim_solve_info(const rfo_sim *s, int *info, int *iters, double *be) {
 
 void rfo_sim_timings(const rfo_sim *s, double *t4) {
     for (int i = 0; i < 4; ++i) t4[i] = s->t4[i];
+}
+
+int rfo_generate_layout(int M, int distribution, double box, double min_dist, unsigned long long seed,
+                        double *positions, double *orientations) {
+    // Centres: rejection sampling against every accepted centre closer than
+    // min_dist, looked up in a grid of cells of side min_dist; uniform in
+    // [0, box)^3 (distribution 0) or isotropic normal with deviation box (1).
+    // Then every orientation: a normal 3-vector (redrawn if |t|^2 < 1e-12),
+    // normalised.  The draws are consumed in that order.
+    if (M < 1 || !positions || !orientations || !(box > 0.0) || min_dist < 0.0 ||
+        (distribution != 0 && distribution != 1))
+        return -1;
+    if (distribution == 0) {
+        const double r = 0.5 * min_dist;
+        if ((double)M * (4.0 / 3.0) * M_PI * std::pow(r, 3.0) > 0.5 * box * box * box) return -1;
+    }
+    LayoutRng rng(seed);
+    const double side = min_dist > 0.0 ? min_dist : 1.0;
+    const double lim = min_dist * min_dist;
+    std::map<std::array<int, 3>, std::vector<int>> cells;
+    const long long budget = (long long)M * 100000;
+    long long tries = 0;
+    for (int count = 0; count < M;) {
+        if (++tries > budget) return -1;
+        double c[3];
+        for (double &v : c) v = distribution == 0 ? box * rng.u01() : box * rng.gauss();
+        const std::array<int, 3> cell = {(int)std::floor(c[0] / side), (int)std::floor(c[1] / side),
+                                         (int)std::floor(c[2] / side)};
+        bool accept = true;
+        if (min_dist > 0.0) {
+            for (int a = -1; a <= 1 && accept; ++a)
+                for (int bb = -1; bb <= 1 && accept; ++bb)
+                    for (int cc = -1; cc <= 1 && accept; ++cc) {
+                        const auto it = cells.find({cell[0] + a, cell[1] + bb, cell[2] + cc});
+                        if (it == cells.end()) continue;
+                        for (const int j : it->second) {
+                            const double dx = c[0] - positions[3 * j], dy = c[1] - positions[3 * j + 1],
+                                         dz = c[2] - positions[3 * j + 2];
+                            if (dx * dx + dy * dy + dz * dz < lim) {
+                                accept = false;
+                                break;
+                            }
+                        }
+                    }
+        }
+        if (!accept) continue;
+        std::copy(c, c + 3, positions + 3 * count);
+        cells[cell].push_back(count);
+        ++count;
+    }
+    for (int i = 0; i < M; ++i) {
+        double t[3], q;
+        do {
+            q = 0.0;
+            for (double &v : t) {
+                v = rng.gauss();
+                q += v * v;
+            }
+        } while (q < 1e-12);
+        q = std::sqrt(q);
+        for (int a = 0; a < 3; ++a) orientations[3 * i + a] = t[a] / q;
+    }
+    return 0;
 }
 
 }  // extern "C"

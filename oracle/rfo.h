@@ -73,6 +73,13 @@ rfo_sim *rfo_sim_create(const rfo_params *p, const double *X0, const double *T0)
 void rfo_sim_destroy(rfo_sim *s);
 /* one time step; step_index 0 is the forward-Euler step */
 int rfo_sim_step(rfo_sim *s);
+/* The same step in parts, for timing one whole step in bounded pieces:
+ * rfo_sim_assemble_part assembles the rows of A and b of target fibers
+ * [i0, i1) into the step's system (held by the handle, n x n); once every
+ * target's rows are in, rfo_sim_finish_step solves, computes the velocities,
+ * advects and rotates the state.  rfo_sim_step = both over all targets. */
+int rfo_sim_assemble_part(rfo_sim *s, int i0, int i1);
+int rfo_sim_finish_step(rfo_sim *s);
 /* outputs of the last step (any pointer may be NULL) */
 void rfo_sim_last(const rfo_sim *s, double *b, double *coeffs, double *V, double *W,
                   double *X, double *T);
@@ -90,6 +97,15 @@ int rfo_assemble_rows(const rfo_params *p, const double *X, const double *T,
 /* velocities of target fibers [i0, i1) only */
 int rfo_velocities_rows(const rfo_params *p, const double *X, const double *T,
                         const double *coeffs, int i0, int i1, double *V, double *W);
+
+/* Seeded synthetic layout: the product's generator (rf_generate_layout)
+ * restated on the oracle side, so that the CPU baseline builds its input
+ * without loading the product library; identical output bit for bit.
+ * distribution 0: centres uniform in [0, box)^3; 1: isotropic normal with
+ * deviation box; minimum centre distance by rejection; orientations
+ * uniform on the sphere.  Returns 0, or -1 for invalid arguments. */
+int rfo_generate_layout(int M, int distribution, double box, double min_dist, unsigned long long seed,
+                        double *positions, double *orientations);
 
 #ifdef __cplusplus
 }

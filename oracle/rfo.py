@@ -68,6 +68,10 @@ def lib():
         L.rfo_sim_last.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]
         L.rfo_sim_solve_info.argtypes = [ctypes.c_void_p, _ip, _ip, _dp]
         L.rfo_sim_timings.argtypes = [ctypes.c_void_p, _dp]
+        L.rfo_sim_assemble_part.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]
+        L.rfo_sim_finish_step.argtypes = [ctypes.c_void_p]
+        L.rfo_generate_layout.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_ulonglong, _dp, _dp]
         _lib = L
     return _lib
 
@@ -183,6 +187,19 @@ def velocities_rows(params, X, T, coeffs, i0, i1):
     return V, W
 
 
+def generate_layout(M, distribution="uniform", box=5.0, min_dist=0.2, seed=1000):
+    """Seeded synthetic layout, bit-identical to the product's generator
+    (centres uniform in [0, box)^3 or isotropic normal with deviation box,
+    minimum centre distance by rejection, orientations uniform on the sphere)."""
+    pos = np.zeros(3 * M)
+    ori = np.zeros(3 * M)
+    dist = {"uniform": 0, "gaussian": 1}[distribution]
+    rc = lib().rfo_generate_layout(M, dist, box, min_dist, seed, _ptr(pos), _ptr(ori))
+    if rc != 0:
+        raise ValueError(f"invalid layout request: M={M} {distribution} box={box} min_dist={min_dist}")
+    return pos.reshape(M, 3), ori.reshape(M, 3)
+
+
 class Simulation:
     """Oracle time stepper: advect_fibers.f90:437-593 over any number of steps."""
 
@@ -195,6 +212,16 @@ class Simulation:
 
     def step(self):
         return lib().rfo_sim_step(self._h)
+
+    def assemble_part(self, i0, i1):
+        """Rows of the current step's system for target fibers [i0, i1)."""
+        rc = lib().rfo_sim_assemble_part(self._h, i0, i1)
+        assert rc == 0, rc
+        return rc
+
+    def finish_step(self):
+        """Solve, velocities and advection of the system assembled by the parts."""
+        return lib().rfo_sim_finish_step(self._h)
 
     def last(self):
         M, N = self.params.M, self.params.N

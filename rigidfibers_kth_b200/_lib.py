@@ -119,6 +119,7 @@ def lib():
         "rf_get_coeffs": (ctypes.c_int, [_h, _dp]),
         "rf_get_rhs": (ctypes.c_int, [_h, _dp]),
         "rf_get_matrix": (ctypes.c_int, [_h, _dp]),
+        "rf_get_matrix_rows": (ctypes.c_int, [_h, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _dp]),
         "rf_matvec": (ctypes.c_int, [_h, _dp, _dp]),
         "rf_matvec_free": (ctypes.c_int, [_h, _dp, _dp]),
         "rf_get_solve_stats": (ctypes.c_int, [_h, ctypes.POINTER(RfSolveStats)]),

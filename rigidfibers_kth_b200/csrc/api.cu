@@ -931,6 +931,30 @@ rf_status rf_get_matrix(rf_handle *h, double *A) {
     return RF_OK;
 }
 
+rf_status rf_get_matrix_rows(rf_handle *h, int32_t which, int64_t row0, int64_t rows, double *out) {
+    if (!h || !out) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    if (which != 0 && which != 1) return rf::fail(h, RF_ERR_INVALID_ARG, "which must be 0 or 1");
+    if (row0 < 0 || rows < 1 || row0 + rows > h->n) return rf::fail(h, RF_ERR_INVALID_ARG, "rows out of range");
+    if (!h->assembled) return rf::fail(h, RF_ERR_INVALID_ARG, "no assembled system");
+    CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    double *dev = nullptr;
+    const size_t bytes = sizeof(double) * (size_t)rows * (size_t)h->n;
+    CK(h, cudaMalloc(&dev, bytes), "row block");
+    cudaError_t e;
+    if (which == 1 && h->A16)
+        e = rf::launch_gather_rows<__nv_bfloat16>(h->A16, h->lda, row0, rows, h->n, dev, h->stream);
+    else if (h->A64)
+        e = rf::launch_gather_rows<double>(h->A64, h->lda, row0, rows, h->n, dev, h->stream);
+    else
+        e = rf::launch_gather_rows<float>(h->A32, h->lda, row0, rows, h->n, dev, h->stream);
+    h->launches += 1;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dev, bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dev);
+    CK(h, e, "download row block");
+    return RF_OK;
+}
+
 rf_status rf_matvec(rf_handle *h, const double *x, double *y) {
     if (!h || !x || !y) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
     CK(h, cudaSetDevice(h->device), "cudaSetDevice");

@@ -369,6 +369,18 @@ __global__ void convert_kernel(int64_t n, const TI *x, TO *y) {
         y[e] = (TO)x[e];
 }
 
+// out[r + c * rows] = A[row0 + r + c * lda] for r < rows, c < cols (FP64 copy
+// of a row block of a column-major matrix in any storage precision)
+template <typename T>
+__global__ void gather_rows_kernel(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols,
+                                   double *out) {
+    const int64_t tot = rows * cols;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = e / rows, r = e - c * rows;
+        out[e] = (double)A[row0 + r + c * lda];
+    }
+}
+
 template <typename T>
 __global__ void block_apply_kernel(int M, int nb, const float *B, const T *v, T *z) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -463,6 +475,12 @@ cudaError_t launch_convert(int64_t n, const TI *x, TO *y, cudaStream_t st) {
     return cudaGetLastError();
 }
 template <typename T>
+cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols, double *out,
+                               cudaStream_t st) {
+    gather_rows_kernel<T><<<grid_for(rows * cols), 256, 0, st>>>(A, lda, row0, rows, cols, out);
+    return cudaGetLastError();
+}
+template <typename T>
 cudaError_t launch_block_apply(int M, int nb, const float *B, const T *v, T *z, cudaStream_t st) {
     const int64_t tot = (int64_t)M * nb;
     block_apply_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(M, nb, B, v, z);
@@ -495,6 +513,12 @@ template cudaError_t launch_convert<float, double>(int64_t, const double *, floa
 template cudaError_t launch_convert<double, float>(int64_t, const float *, double *, cudaStream_t);
 template cudaError_t launch_convert<double, __nv_bfloat16>(int64_t, const __nv_bfloat16 *, double *,
                                                            cudaStream_t);
+template cudaError_t launch_gather_rows<double>(const double *, int64_t, int64_t, int64_t, int64_t, double *,
+                                                cudaStream_t);
+template cudaError_t launch_gather_rows<float>(const float *, int64_t, int64_t, int64_t, int64_t, double *,
+                                               cudaStream_t);
+template cudaError_t launch_gather_rows<__nv_bfloat16>(const __nv_bfloat16 *, int64_t, int64_t, int64_t, int64_t,
+                                                       double *, cudaStream_t);
 template cudaError_t launch_block_apply<double>(int, int, const float *, const double *, double *, cudaStream_t);
 template cudaError_t launch_block_apply<float>(int, int, const float *, const float *, float *, cudaStream_t);
 

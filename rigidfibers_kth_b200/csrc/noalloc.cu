@@ -7,7 +7,9 @@
 // loop that must not stall, since cudaMalloc and cudaFree can synchronise the
 // device.  Such callers hand in their own device buffers for A, x and y; the
 // partial sums the product needs live in one fixed array inside this
-// library, reserved when the library is loaded.
+// library.  With CUDA's default lazy module loading the driver reserves the
+// array on a device when this file's device code is first used there: at the
+// cudaGetSymbolAddress of the first call on that device.
 //
 // The product is the streaming column-major GEMV of the solver (linalg.cu):
 // column ranges are split across the grid and the per-split partial sums are
@@ -20,8 +22,8 @@
 
 namespace {
 
-// 8 MiB of partial sums (1,048,576 doubles).  Every GPU that loads the
-// library keeps this array resident until the process exits.
+// 8 MiB of partial sums (1,048,576 doubles).  Every GPU on which the entry
+// point has been called keeps this array resident until the process exits.
 constexpr int64_t kScratchDoubles = 1 << 20;
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 

@@ -174,6 +174,10 @@ cudaError_t launch_axpy_fd(int64_t n, double alpha, const float *d, double *x, c
 // convert
 template <typename TO, typename TI>
 cudaError_t launch_convert(int64_t n, const TI *x, TO *y, cudaStream_t st);
+// FP64 copy of rows [row0, row0 + rows) of a column-major matrix (cols columns)
+template <typename T>
+cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols, double *out,
+                               cudaStream_t st);
 
 // ---- block-diagonal preconditioner (15x15 blocks per fiber, FP32) -------------
 // z = blockdiag(B) v, B[i] row-major 3N x 3N

@@ -231,6 +231,13 @@ class Simulation:
         L.check(L.lib().rf_get_matrix(self._h, _ptr(A)), self._h)
         return A
 
+    def matrix_rows(self, row0, rows, inner=False):
+        """Rows [row0, row0 + rows) of the stored matrix as an FP64 (rows, n)
+        array; inner=True reads the inner solve's copy (BF16 where stored)."""
+        A = np.zeros((rows, self.n), order="F")
+        L.check(L.lib().rf_get_matrix_rows(self._h, int(bool(inner)), row0, rows, _ptr(A)), self._h)
+        return A
+
     def matvec(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.zeros(self.n)

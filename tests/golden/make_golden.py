@@ -11,7 +11,7 @@ GMRES restart 10, 100 iterations, tol 1e-5, ExtForce (0,0,-1).
 This script reads those files from a checkout of the reference and writes one
 compressed npz, so the tests never need the reference at run time.
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py PATH_TO_REFERENCE_CHECKOUT
 """
 import os
 import sys
@@ -45,4 +45,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py PATH_TO_REFERENCE_CHECKOUT")
+    main(sys.argv[1])

@@ -70,10 +70,11 @@ def test_two_gloo_ranks_barrier_and_max_over_ranks():
 def test_reference_arm_json_line_contract():
     """`bench.py --impl reference` on one process (a small M keeps it short):
     one JSON line with the contract's keys, the CPU baseline describing the
-    run and an end-to-end figure without host-device traffic."""
+    run, an end-to-end figure without host-device traffic, the same `config`
+    as the product arm, and the timed parts adding up to one whole step."""
     env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--M", "40",
-                        "--steps", "1", "--warmup", "0"], cwd=ROOT, env=env, capture_output=True, text=True,
+                        "--steps", "4", "--warmup", "3"], cwd=ROOT, env=env, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stderr
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
@@ -85,3 +86,25 @@ def test_reference_arm_json_line_contract():
     assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # K parts of one step: value = 1 step / (K x mean part time)
+    assert abs(d["value"] * d["steps"] * d["ms_per_step"] * 1e-3 - 1.0) < 1e-9
+    assert d["arm"]["gmres"]["info"] == 0 and d["arm"]["gmres"]["residual"] <= 1e-10
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert d["config"] == bench.workload_config(40, 1)
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """The reference arm must not map the product library: its layout comes
+    from the oracle's restatement of the generator."""
+    code = ("import json, sys; sys.path.insert(0, {root!r}); import bench; "
+            "sys.argv = ['bench.py', '--impl', 'reference', '--M', '20', '--steps', '1', '--warmup', '0']; "
+            "out = bench.run_reference(bench.parse_args()); maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({{'ok': out is not None, 'product': 'librigidfibers' in maps, "
+            "'oracle': 'librfo' in maps}}))").format(root=ROOT)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    d = json.loads(r.stdout.strip().splitlines()[-1])
+    assert d == {"ok": True, "product": False, "oracle": True}

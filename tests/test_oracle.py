@@ -111,3 +111,45 @@ def test_flop_count_of_the_reference_assembly():
     near = 0.069
     mixed = near * (fwd["add"] + fwd["mul"]) + (1 - near) * (bwd["add"] + bwd["mul"])
     assert abs(mixed - bench.ASM_FLOPS_PER_PAIR) < 1.0
+
+
+@pytest.mark.parametrize("case", ["100_analytic_gmres", "100_numeric_direct"])
+def test_step_in_parts_equals_whole_step(golden, case):
+    """The CPU baseline times one whole step as row slices of the assembly
+    followed by the rest of the step; the parts give the whole step's
+    results bit for bit, over two steps (Euler, then multistep)."""
+    X0, T0 = golden["layout_pos"], golden["layout_orient"]
+    p = rfo.make_params(100, analytic="analytic" in case, direct="direct" in case)
+    whole = rfo.Simulation(p, X0, T0)
+    parts = rfo.Simulation(p, X0, T0)
+    for step in (0, 1):
+        assert whole.step() == 0
+        for i0, i1 in [(0, 13), (13, 13), (13, 60), (60, 99), (99, 100)]:
+            parts.assemble_part(i0, i1)
+        assert parts.finish_step() == 0
+        a, b = whole.last(), parts.last()
+        for q in QUANTITIES:
+            assert np.array_equal(a[q], b[q]), (step, q)
+        for q in QUANTITIES:
+            assert np.abs(b[q] - golden[f"{case}/{step}_{q}"]).max() <= GOLDEN_ATOL
+
+
+def test_oracle_layout_matches_product_generator_bit_for_bit():
+    """rfo.generate_layout (oracle side, used by the CPU baseline so that it
+    never loads the product library) reproduces rf_generate_layout exactly,
+    for both distributions and the benchmark configurations' seeds.  The
+    product call is host code of librigidfibers.so: no GPU is needed."""
+    import rigidfibers_kth_b200 as rf
+
+    for M, dist, box, seed in [(100, "uniform", 2.5, 1001), (1000, "uniform", 5.0, 1002),
+                               (2000, "uniform", 6.5, 1003), (4000, "gaussian", 3.0, 1004),
+                               (8000, "uniform", 10.0, 1005), (333, "gaussian", 1.0, 7), (50, "uniform", 1.0, 0)]:
+        po, oo = rfo.generate_layout(M, dist, box, 0.2, seed)
+        pg, og = rf.generate_layout(M, dist, box, 0.2, seed)
+        assert np.array_equal(po, pg) and np.array_equal(oo, og), (M, dist, seed)
+        d = np.linalg.norm(po[:, None, :] - po[None, :, :], axis=2) if M <= 1000 else None
+        if d is not None:
+            assert d[~np.eye(M, dtype=bool)].min() >= 0.2
+        assert np.allclose(np.linalg.norm(oo, axis=1), 1.0, atol=1e-15)
+    with pytest.raises(ValueError):
+        rfo.generate_layout(10**6, "uniform", 1.0, 0.2, 1)  # cannot be packed
