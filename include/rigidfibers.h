@@ -65,8 +65,10 @@ typedef enum rf_precision {
 
 typedef enum rf_preconditioner {
     RF_PC_NONE = 0,          /* block-Jacobi on the fiber's own 15x15 block == identity here */
-    RF_PC_CLUSTER = 1,       /* exact fiber block of the inverse of its k-NN cluster submatrix */
-    RF_PC_LEARNED = 2        /* MLP-corrected block (see rf_pc_* below); falls back to RF_PC_NONE */
+    RF_PC_CLUSTER = 1,       /* z_i = v_i + sum_m B_im v_(m-th neighbour), B_im the exact coupling blocks
+                                of the inverse of the fiber's k-NN cluster submatrix (first block row) */
+    RF_PC_LEARNED = 2        /* the same form with B_im predicted by the MLP below; falls back to
+                                RF_PC_NONE without weights */
 } rf_preconditioner;
 
 typedef enum rf_velocity_mode {
@@ -95,7 +97,7 @@ typedef struct rf_params {
     int32_t velocity_mode;               /* rf_velocity_mode */
     int32_t device;                      /* CUDA device ordinal */
     int32_t max_refinements;             /* mixed precision: outer refinement steps (default 30) */
-    int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 12) */
+    int32_t cluster_size;                /* RF_PC_CLUSTER: neighbours per cluster (default 8) */
     double inner_tol;                    /* mixed precision: the deepest reduction one inner GMRES solve
                                             is asked for (default 1e-3); the refinements are planned as the
                                             fewest that reach gmres_tol with inner solves no deeper than
@@ -235,24 +237,30 @@ rf_status rf_generate_layout(int32_t M, int32_t distribution, double box, double
 double rf_min_segment_distance(int32_t M, const double *positions, const double *orientations);
 
 /* ---- Learned preconditioner (benchmark addition; no reference counterpart)
- * MLP: features of the k=16 nearest neighbours in the fiber's own frame
- * (e3 = its orientation, e1 toward the nearest neighbour): per neighbour the
- * relative centre (3) and the six products u_a u_b of its orientation
- * (sign-invariant), 16 x 9 floats -> 256 -> 256 -> 225, ReLU, predicting the
- * fiber's 15 x 15 block minus the identity in that frame.
+ * z_i = v_i + sum_{m < 8} B_im v_(m-th nearest neighbour of i).  The MLP
+ * predicts each coupling block B_im (15 x 15) from the features of the pair:
+ * the 16 nearest neighbours of fiber i in its own frame (e3 = its
+ * orientation, e1 toward the nearest neighbour), 9 floats each, neighbour m
+ * first (relative centre, orientation with a canonical sign, orientation
+ * squared), then the other 15 nearest first (relative centre and the six
+ * products u_a u_b of the orientation), 16 x 9 floats -> 256 -> 256 -> 225,
+ * ReLU.  The output is the block in fiber i's frame with the columns of odd
+ * Legendre order multiplied by neighbour m's canonical sign.
  * Weights are FP32, layer-major: W1[256x144] b1[256] W2[256x256] b2[256]
  * W3[225x256] b3[225] (row-major, out x in). */
 #define RF_MLP_K 16
+#define RF_MLP_PAIRS 8
 #define RF_MLP_IN (RF_MLP_K * 9)
 #define RF_MLP_HIDDEN 256
 #define RF_MLP_OUT 225
 int64_t rf_mlp_num_params(void);
 /* Install weights used by RF_PC_LEARNED. */
 rf_status rf_set_mlp_weights(rf_handle *h, const float *weights, int64_t count);
-/* Features (M x 144) of the current state. */
+/* Pair features ((M * 8) x 144, fiber-major, neighbour-minor) of the current state. */
 rf_status rf_compute_features(rf_handle *h, float *features);
-/* Exact cluster block inverses minus identity (M x 225, row-major 15x15 per
- * fiber) of the current assembled system: the training targets. */
+/* Exact coupling blocks of the current assembled system ((M * 8) x 225,
+ * row-major 15 x 15, same order as the features), in the frame and sign
+ * convention of the MLP output: the training targets.  Needs cluster_size >= 8. */
 rf_status rf_compute_cluster_targets(rf_handle *h, float *targets);
 
 /* Stand-alone trainer on the device: owns weights, Adam state and a dataset. */

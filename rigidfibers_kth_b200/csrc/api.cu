@@ -221,7 +221,7 @@ void rf_params_default(rf_params *p) {
     p->velocity_mode = RF_VEL_RECOMPUTE;
     p->device = 0;
     p->max_refinements = 30;
-    p->cluster_size = 12;
+    p->cluster_size = 8;
     p->inner_tol = 1e-3;
     p->near_field_c = 6.0;
 }
@@ -654,7 +654,8 @@ rf_status rf_solve_system(rf_handle *h) {
             });
         };
         rf::Gmres<double>::Op P = [h, nb](const double *in, double *out) {
-            return rf::launch_block_apply<double>(h->M, nb, h->Pblocks, in, out, h->stream);
+            return rf::launch_pair_apply<double>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+                                                  h->stream);
         };
         CK(h, h->gm64->solve(A, use_pc ? &P : nullptr, h->b, h->x, false, tol, maxit, &res), "GMRES");
         if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
@@ -672,7 +673,8 @@ rf_status rf_solve_system(rf_handle *h) {
             });
         };
         rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
-            return rf::launch_block_apply<float>(h->M, nb, h->Pblocks, in, out, h->stream);
+            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+                                                 h->stream);
         };
         CK(h, (rf::launch_convert<float, double>(h->n, h->x, h->x32, st)), "convert");
         CK(h, (rf::launch_convert<float, double>(h->n, h->b, h->r32, st)), "convert");
@@ -703,8 +705,32 @@ rf_status rf_solve_system(rf_handle *h) {
             });
         };
         rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
-            return rf::launch_block_apply<float>(h->M, nb, h->Pblocks, in, out, h->stream);
+            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+                                                 h->stream);
         };
+        // the same operators for the device-controlled inner solve: their
+        // kernels return at once once the solve has stopped
+        rf::Gmres<float>::StopOp Alo_s = [h, bf16](const float *in, float *out, const int *stop) {
+            h->launches += 2;
+            return timed_product(h, (bf16 ? 2.0 : 4.0) * h->lda * h->n, [&] {
+                if (bf16)
+                    return rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, h->n, h->n, in, out,
+                                                                               nullptr, h->work32, h->work_elems,
+                                                                               h->sm_count, h->stream, stop);
+                return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
+                                                                   h->work32, h->work_elems, h->sm_count, h->stream,
+                                                                   stop);
+            });
+        };
+        rf::Gmres<float>::StopOp P_s = [h, nb](const float *in, float *out, const int *stop) {
+            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+                                                 h->stream, stop);
+        };
+        // a product queued after the inner solve stopped returns at once: not a product to time
+        auto drop_skipped = [h] {
+            if (h->gt.on && h->gt.used >= 2) h->gt.used -= 2;
+        };
+        const bool device_control = m <= rf::kArnoldiMax;
         double *dnorm = h->dscal;
         const rf::RedBuf &rb = h->rb;
         auto norm_of = [&](const double *v, double *hv) -> cudaError_t {
@@ -763,7 +789,11 @@ rf_status rf_solve_system(rf_handle *h) {
             const double need = 0.5 * tol * bn / rn;
             const int left = std::max(1, (int)std::ceil(std::log(need) / std::log(itol) - 1e-9));
             const double itol_k = std::min(0.5, std::pow(need, 1.0 / left));
-            e = h->gm32->solve(Alo, use_pc ? &P : nullptr, h->r32, h->d32, true, itol_k, maxit, &res, false);
+            if (device_control)
+                e = h->gm32->solve_device(Alo_s, use_pc ? &P_s : nullptr, h->r32, h->d32, itol_k, maxit, &res,
+                                          drop_skipped);
+            else
+                e = h->gm32->solve(Alo, use_pc ? &P : nullptr, h->r32, h->d32, true, itol_k, maxit, &res, false);
             if (e != cudaSuccess) break;
             if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
             h->launches += res.launches;

@@ -2,6 +2,7 @@
 #include "gmres.h"
 
 #include <cmath>
+#include <cstring>
 
 namespace rf {
 
@@ -48,6 +49,11 @@ Gmres<VT>::~Gmres() {
     cudaFree(rb_.partials);
     cudaFree(rb_.counter);
     if (hpin_) cudaFreeHost(hpin_);
+    cudaFree(ctrl_);
+    cudaFree(cpart_);
+    if (hstat_) cudaFreeHost(hstat_);
+    for (cudaEvent_t ev : step_ev_)
+        if (ev) cudaEventDestroy(ev);
 }
 
 template <typename VT>
@@ -70,7 +76,107 @@ cudaError_t Gmres<VT>::init(int64_t n, int m, cudaStream_t st) {
     H_.assign((size_t)(m + 1) * (m + 1), 0.0);
     cs_.assign(m, 0.0);
     sn_.assign(m, 0.0);
+    if (m <= kArnoldiMax) {
+        RF_TRY(cudaMalloc(&ctrl_, sizeof(ArnoldiCtrl)));
+        RF_TRY(cudaMemsetAsync(ctrl_, 0, sizeof(ArnoldiCtrl), st));
+        RF_TRY(cudaMalloc(&cpart_, sizeof(double) * kArnoldiMax * rb_.max_blocks));
+        RF_TRY(cudaHostAlloc(&hstat_, sizeof(ArnoldiStat) * (kArnoldiMax + 1), cudaHostAllocMapped));
+        std::memset(hstat_, 0, sizeof(ArnoldiStat) * (kArnoldiMax + 1));
+        RF_TRY(cudaHostGetDevicePointer((void **)&dstat_, hstat_, 0));
+        for (cudaEvent_t &ev : step_ev_) RF_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    }
     return cudaStreamSynchronize(st);
+}
+
+template <typename VT>
+cudaError_t Gmres<VT>::solve_device(const StopOp &A, const StopOp *P, const VT *b, VT *x, double tol, int max_iters,
+                                    GmresResult *res, const std::function<void()> &on_skipped_product) {
+    *res = GmresResult();
+    const int m = m_;
+    if (!ctrl_ || m > kArnoldiMax) return cudaErrorInvalidValue;
+    const int iterMax = max_iters > 0 ? max_iters : (int)n_;
+    const int *stop = &ctrl_->stop;
+    volatile ArnoldiStat *hs = hstat_;
+    RF_TRY(cudaMemsetAsync(x, 0, sizeof(VT) * n_, st_));
+    RF_TRY(launch_arnoldi_start<VT>(n_, b, V_, ctrl_, tol, iterMax, 1, cpart_, rb_.counter, rb_.max_blocks,
+                                    dstat_ + kArnoldiMax, st_));
+    res->launches += 3;
+    int last_stop = 0;
+    for (;;) {
+        // the start of a cycle may already stop the solve (zero or non-finite
+        // residual): learn that before queuing steps
+        RF_TRY(cudaStreamSynchronize(st_));
+        last_stop = hs[kArnoldiMax].stop;
+        if (last_stop == 3) {
+            res->info = kInfoNaN;
+            return cudaSuccess;
+        }
+        if (last_stop) {
+            res->info = 0;
+            return cudaSuccess;
+        }
+        bool ahead = false;  // a step was queued after the one that stopped
+        for (int j = 0; j < m; ++j) {
+            const VT *in = V_ + (size_t)j * n_;
+            if (P) {
+                RF_TRY((*P)(in, z_, stop));
+                res->launches++;
+                in = z_;
+            }
+            RF_TRY(A(in, w_, stop));
+            res->matvecs++;
+            RF_TRY(launch_arnoldi_orthogonalize<VT>(n_, w_, V_, j, m, ctrl_, dstat_, cpart_, rb_.counter,
+                                                    rb_.max_blocks, st_));
+            res->launches += 4;
+            RF_TRY(cudaEventRecord(step_ev_[j], st_));
+            if (j > 0) {
+                // step j is queued: now wait for step j - 1 (the GPU is busy with j)
+                RF_TRY(cudaEventSynchronize(step_ev_[j - 1]));
+                last_stop = hs[j - 1].stop;
+                res->iterations = hs[j - 1].itn;
+                res->backward_error = hs[j - 1].bea;
+                if (last_stop) {
+                    ahead = true;
+                    break;
+                }
+            }
+        }
+        if (!ahead) {
+            RF_TRY(cudaEventSynchronize(step_ev_[m - 1]));
+            last_stop = hs[m - 1].stop;
+            res->iterations = hs[m - 1].itn;
+            res->backward_error = hs[m - 1].bea;
+        } else {
+            res->matvecs--;  // the queued step's product returned at once
+            if (on_skipped_product) on_skipped_product();
+        }
+        if (last_stop == 3) {
+            res->info = kInfoNaN;
+            return cudaSuccess;
+        }
+        // x += P (V y) over the steps of this cycle
+        RF_TRY(launch_arnoldi_combine<VT>(n_, V_, ctrl_, u_, st_));
+        res->launches += 2;
+        const VT *upd = u_;
+        if (P) {
+            RF_TRY((*P)(u_, z_, nullptr));
+            upd = z_;
+            res->launches++;
+        }
+        RF_TRY(launch_add<VT>(n_, x, upd, x, st_));
+        res->launches++;
+        if (last_stop) {
+            res->info = last_stop == 1 ? 0 : -4;
+            return cudaSuccess;
+        }
+        // restart from the residual of the updated x
+        RF_TRY(A(x, w_, nullptr));
+        res->matvecs++;
+        RF_TRY(launch_bmr<VT>(n_, b, w_, st_));
+        RF_TRY(launch_arnoldi_start<VT>(n_, w_, V_, ctrl_, tol, iterMax, 0, cpart_, rb_.counter, rb_.max_blocks,
+                                        dstat_ + kArnoldiMax, st_));
+        res->launches += 4;
+    }
 }
 
 template <typename VT>

@@ -6,7 +6,8 @@
 // residual <= tol" on ||b - A x|| / ||b||.  Right preconditioning z = P v is
 // optional (the residual keeps its meaning).  Krylov vectors live on the
 // device in VT (double or float); the Hessenberg matrix, rotations and the
-// least-squares solve are FP64 on the host (a few hundred flops per step).
+// least-squares solve are FP64 on the host (a few hundred flops per step);
+// solve_device keeps them on the device (arnoldi.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -32,6 +33,8 @@ template <typename VT>
 class Gmres {
    public:
     using Op = std::function<cudaError_t(const VT *in, VT *out)>;
+    // an operator whose kernels return at once when *stop != 0 (stop may be null)
+    using StopOp = std::function<cudaError_t(const VT *in, VT *out, const int *stop)>;
 
     Gmres() = default;
     ~Gmres();
@@ -42,6 +45,14 @@ class Gmres {
     // solves of iterative refinement, whose caller recomputes the residual).
     cudaError_t solve(const Op &A, const Op *P, const VT *b, VT *x, bool x_is_zero, double tol, int max_iters,
                       GmresResult *res, bool check_true = true);
+    // Inner solve of the refinement, controlled on the device (arnoldi.cu):
+    // x = 0 initially, stop on the Arnoldi estimate <= tol or the budget,
+    // CGS2 orthogonalisation.  The host queues each step before it learns
+    // whether the previous one stopped; a step queued after the stop runs as
+    // empty launches, and `on_skipped_product` is called once for its
+    // product (the caller's product timer drops it).  Needs m <= kArnoldiMax.
+    cudaError_t solve_device(const StopOp &A, const StopOp *P, const VT *b, VT *x, double tol, int max_iters,
+                             GmresResult *res, const std::function<void()> &on_skipped_product);
     int restart() const { return m_; }
 
    private:
@@ -62,6 +73,12 @@ class Gmres {
     double *ydev_ = nullptr;   // m
     double *hpin_ = nullptr;   // pinned host mirror of hcol
     RedBuf rb_{};
+    // device-controlled solve
+    ArnoldiCtrl *ctrl_ = nullptr;     // device
+    ArnoldiStat *hstat_ = nullptr;    // host-mapped, one per step of a cycle, then the cycle start
+    ArnoldiStat *dstat_ = nullptr;    // its device address
+    double *cpart_ = nullptr;         // kArnoldiMax x max_blocks partial sums
+    cudaEvent_t step_ev_[kArnoldiMax] = {};
     std::vector<double> H_;    // (m+1) x (m+1) column-major, column m = rhs g
     std::vector<double> cs_, sn_;
 };

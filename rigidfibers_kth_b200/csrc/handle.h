@@ -81,12 +81,13 @@ struct rf_handle {
     double *hscal = nullptr;   // pinned host mirror
     rf::RedBuf rb{};
     // preconditioner
-    float *Pblocks = nullptr;  // M x (3N)^2 row-major blocks
+    float *Pblocks = nullptr;  // M x RF_MLP_PAIRS coupling blocks, (3N)^2 row-major each
     bool pc_ready = false;
-    int *knn = nullptr;        // M x kmax neighbour lists
+    int pc_pairs = 0;          // coupling blocks in use per fiber
+    int *knn = nullptr;        // M x RF_MLP_K neighbour lists, nearest first
     float *mlp_w = nullptr;    // MLP weights on the device
     bool mlp_loaded = false;
-    float *feat = nullptr;     // M x 144 features
+    float *feat = nullptr;     // (M x RF_MLP_PAIRS) x 144 pair features, M x 9 frames, M x RF_MLP_PAIRS signs
     float *mlp_h1 = nullptr, *mlp_h2 = nullptr, *mlp_out = nullptr;
 
     // live timing of the inner-solve products (rf_gemv_timer)

@@ -76,7 +76,8 @@ template <typename S, typename X, typename ACC>
 __global__ void __launch_bounds__(kGemvThreads) gemv_partial_kernel(const S *__restrict__ A, int64_t lda, int64_t m,
                                                                     int64_t k, const X *__restrict__ x,
                                                                     int64_t cols_per_split, ACC *__restrict__ work,
-                                                                    int64_t mpad) {
+                                                                    int64_t mpad, const int *__restrict__ stop) {
+    if (stop && *stop) return;  // a speculatively queued product of a finished solve
     constexpr int VEC = Vec16<S>::kVec;
     const int64_t row = ((int64_t)blockIdx.x * kGemvThreads + threadIdx.x) * VEC;
     const int64_t c0 = (int64_t)blockIdx.y * cols_per_split;
@@ -120,7 +121,8 @@ __global__ void __launch_bounds__(kGemvThreads) gemv_partial_kernel(const S *__r
 
 template <typename ACC, typename Y>
 __global__ void gemv_reduce_kernel(const ACC *__restrict__ work, int splits, int64_t mpad, int64_t m, Y *y,
-                                   const Y *r) {
+                                   const Y *r, const int *__restrict__ stop) {
+    if (stop && *stop) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     ACC s = (ACC)0;
@@ -181,7 +183,7 @@ int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes) {
 
 template <typename S, typename X, typename ACC, typename Y>
 cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *x, Y *y, const Y *r, ACC *work,
-                        int64_t work_elems, int sm_count, cudaStream_t st) {
+                        int64_t work_elems, int sm_count, cudaStream_t st, const int *stop) {
     constexpr int VEC = Vec16<S>::kVec;
     const int64_t tiles = (lda + (int64_t)kGemvThreads * VEC - 1) / ((int64_t)kGemvThreads * VEC);
     const int64_t mpad = tiles * kGemvThreads * VEC;
@@ -190,30 +192,30 @@ cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *
     if ((int64_t)splits * mpad > work_elems) return cudaErrorInvalidValue;
     const int64_t cps = (k + splits - 1) / splits;
     dim3 grid((unsigned)tiles, (unsigned)splits);
-    gemv_partial_kernel<S, X, ACC><<<grid, kGemvThreads, 0, st>>>(A, lda, m, k, x, cps, work, mpad);
+    gemv_partial_kernel<S, X, ACC><<<grid, kGemvThreads, 0, st>>>(A, lda, m, k, x, cps, work, mpad, stop);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    gemv_reduce_kernel<ACC, Y><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(work, splits, mpad, m, y, r);
+    gemv_reduce_kernel<ACC, Y><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(work, splits, mpad, m, y, r, stop);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_gemv<double, double, double, double>(const double *, int64_t, int64_t, int64_t,
                                                                  const double *, double *, const double *,
-                                                                 double *, int64_t, int, cudaStream_t);
+                                                                 double *, int64_t, int, cudaStream_t, const int *);
 template cudaError_t launch_gemv<float, double, double, double>(const float *, int64_t, int64_t, int64_t,
                                                                 const double *, double *, const double *,
-                                                                double *, int64_t, int, cudaStream_t);
+                                                                double *, int64_t, int, cudaStream_t, const int *);
 template cudaError_t launch_gemv<float, float, float, float>(const float *, int64_t, int64_t, int64_t,
                                                              const float *, float *, const float *, float *,
-                                                             int64_t, int, cudaStream_t);
+                                                             int64_t, int, cudaStream_t, const int *);
 template cudaError_t launch_gemv<__nv_bfloat16, float, float, float>(const __nv_bfloat16 *, int64_t, int64_t,
                                                                      int64_t, const float *, float *,
                                                                      const float *, float *, int64_t, int,
-                                                                     cudaStream_t);
+                                                                     cudaStream_t, const int *);
 template cudaError_t launch_gemv<__nv_bfloat16, double, double, double>(const __nv_bfloat16 *, int64_t, int64_t,
                                                                         int64_t, const double *, double *,
                                                                         const double *, double *, int64_t, int,
-                                                                        cudaStream_t);
+                                                                        cudaStream_t, const int *);
 
 // ---------------------------------------------------------------------------
 // reductions
@@ -381,16 +383,26 @@ __global__ void gather_rows_kernel(const T *A, int64_t lda, int64_t row0, int64_
     }
 }
 
+// z_i = v_i + sum_{m < kp} B_{i,m} v_{j_m}: one thread per output entry (i, r);
+// B row-major blocks, pstride blocks per fiber; j_m = knn[i * kstride + m]
+// (negative: no neighbour).  FP64 accumulation in a fixed order.
 template <typename T>
-__global__ void block_apply_kernel(int M, int nb, const float *B, const T *v, T *z) {
+__global__ void pair_apply_kernel(int M, int nb, int kp, int pstride, const float *__restrict__ B,
+                                  const int *__restrict__ knn, int kstride, const T *__restrict__ v, T *__restrict__ z,
+                                  const int *__restrict__ stop) {
+    if (stop && *stop) return;
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (int64_t)M * nb) return;
     const int64_t i = idx / nb;
     const int r = (int)(idx - i * nb);
-    const float *b = B + (i * nb + r) * nb;
-    const T *vi = v + i * nb;
-    double s = 0.0;
-    for (int c = 0; c < nb; ++c) s += (double)b[c] * (double)vi[c];
+    double s = (double)v[idx];
+    for (int m = 0; m < kp; ++m) {
+        const int j = knn[i * kstride + m];
+        if (j < 0) continue;
+        const float *b = B + ((i * pstride + m) * nb + r) * nb;
+        const T *vj = v + (int64_t)j * nb;
+        for (int c = 0; c < nb; ++c) s += (double)b[c] * (double)vj[c];
+    }
     z[idx] = (T)s;
 }
 
@@ -481,9 +493,11 @@ cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t ro
     return cudaGetLastError();
 }
 template <typename T>
-cudaError_t launch_block_apply(int M, int nb, const float *B, const T *v, T *z, cudaStream_t st) {
+cudaError_t launch_pair_apply(int M, int nb, int kp, int pstride, const float *B, const int *knn, int kstride,
+                              const T *v, T *z, cudaStream_t st, const int *stop) {
     const int64_t tot = (int64_t)M * nb;
-    block_apply_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(M, nb, B, v, z);
+    pair_apply_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(M, nb, kp, pstride, B, knn, kstride, v, z,
+                                                                         stop);
     return cudaGetLastError();
 }
 
@@ -519,7 +533,9 @@ template cudaError_t launch_gather_rows<float>(const float *, int64_t, int64_t, 
                                                cudaStream_t);
 template cudaError_t launch_gather_rows<__nv_bfloat16>(const __nv_bfloat16 *, int64_t, int64_t, int64_t, int64_t,
                                                        double *, cudaStream_t);
-template cudaError_t launch_block_apply<double>(int, int, const float *, const double *, double *, cudaStream_t);
-template cudaError_t launch_block_apply<float>(int, int, const float *, const float *, float *, cudaStream_t);
+template cudaError_t launch_pair_apply<double>(int, int, int, int, const float *, const int *, int, const double *,
+                                               double *, cudaStream_t, const int *);
+template cudaError_t launch_pair_apply<float>(int, int, int, int, const float *, const int *, int, const float *,
+                                              float *, cudaStream_t, const int *);
 
 }  // namespace rf

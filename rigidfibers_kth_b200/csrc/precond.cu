@@ -1,19 +1,31 @@
-// precond.cu - block preconditioners for the right-preconditioned GMRES.
+// precond.cu - neighbour-block preconditioners for the right-preconditioned GMRES.
 //
 // The 3N x 3N diagonal blocks of A are the identity (matrix_assembly.f90:
-// 489-492), so plain block-Jacobi is no preconditioning at all.  The blocks
-// used here approximate the fiber's own block of the inverse instead:
+// 489-492), so plain block-Jacobi is no preconditioning at all, and no
+// block-diagonal correction helps either: the lowest eigenvalues of A belong
+// to modes localised on two or three close fibers (a pair coupled by a block
+// C has eigenvalues 1 +- sigma(C); a block-diagonal P maps them to
+// 1/(1 -+ sigma) and keeps their ratio), the highest to modes spread over
+// tens of fibers in the dense core.  What does help is coupling a fiber to
+// its nearest neighbours:
 //
-//   RF_PC_CLUSTER  B_i = [S_i^-1]_00, S_i = A restricted to fiber i and its
-//                  k nearest neighbours (the "exact local-cluster block
-//                  inverse"); one CTA per fiber factorises S_i in shared
-//                  memory (FP32 LU with partial pivoting).
-//   RF_PC_LEARNED  B_i = I + R_i^T O_i R_i, O_i the output of a small MLP on
-//                  the geometry of the 16 nearest neighbours expressed in a
-//                  frame attached to fiber i (R_i = blockdiag of the frame
-//                  rotation).  The inverse blocks transform as
-//                  B(Q config) = Q B(config) Q^T under rotations Q, so the
-//                  network only learns the rotation-free part.
+//   z_i = v_i + sum_{m < kp} B_{i,m} v_{j_m},   j_m = the m-th nearest neighbour
+//
+// with B_{i,m} the coupling blocks of the local inverse:
+//
+//   RF_PC_CLUSTER  B_{i,m} = [S_i^-1]_{0, m+1}, S_i = A restricted to fiber i
+//                  and its kc nearest neighbours (the exact local-cluster
+//                  inverse); one CTA per fiber factorises S_i^T in shared
+//                  memory (FP32 LU with partial pivoting) and keeps the
+//                  first block row.
+//   RF_PC_LEARNED  B_{i,m} predicted by a small MLP from the geometry of the
+//                  16 nearest neighbours expressed in a frame attached to
+//                  fiber i, neighbour m listed first (one evaluation per
+//                  pair).  Blocks transform as B(Q config) = Q B(config) Q^T
+//                  under rotations Q, and neighbour m's orientation enters
+//                  with a canonical sign (the block's odd-order columns
+//                  change sign with it), so the network only learns the
+//                  rotation- and sign-free part.
 //
 // The MLP (144 -> 256 -> 256 -> 225, ReLU) is trained by the trainer below
 // with hand-written FP32 GEMM kernels (forward and backward) and Adam.
@@ -29,6 +41,7 @@ namespace rf {
 namespace {
 
 constexpr int kK = RF_MLP_K;          // neighbours in the features
+constexpr int kPair = RF_MLP_PAIRS;   // neighbour blocks per fiber
 constexpr int kIn = RF_MLP_IN;        // 144
 constexpr int kHid = RF_MLP_HIDDEN;   // 256
 constexpr int kOut = RF_MLP_OUT;      // 225
@@ -98,14 +111,15 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(int M, const double
     }
 }
 
-// ------------------------------------------------------------------ cluster inverse
-// S = A[C, C] with C = {i, knn_0, .., knn_{kc-1}}; solve S X = E (E = the
+// ------------------------------------------------------------------ cluster inverse rows
+// S = A[C, C] with C = {i, knn_0, .., knn_{kc-1}}; solve S^T X = E (E = the
 // first nb columns of the identity) by LU with partial pivoting in shared
-// memory and keep X[0:nb, 0:nb].
+// memory: X^T is the first block row of S^-1, and its column blocks 1..kp are
+// the couplings B_{i,m} (out[i][m], row-major nb x nb; zero for m >= kp).
 template <typename T>
-__global__ void __launch_bounds__(256) cluster_inverse_kernel(int M, int nb, const T *__restrict__ A, int64_t lda,
-                                                              const int *__restrict__ knn, int K, int kc,
-                                                              float *__restrict__ out, int *__restrict__ singular) {
+__global__ void __launch_bounds__(256) cluster_rows_kernel(int M, int nb, const T *__restrict__ A, int64_t lda,
+                                                           const int *__restrict__ knn, int kstride, int kc, int kp,
+                                                           float *__restrict__ out, int *__restrict__ singular) {
     extern __shared__ float sm[];
     __shared__ int s_fib[32];
     __shared__ int s_piv;
@@ -115,14 +129,14 @@ __global__ void __launch_bounds__(256) cluster_inverse_kernel(int M, int nb, con
     const int w = s + nb;       // augmented width
     const int ld = w + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
-    if (tid <= kc) s_fib[tid] = tid == 0 ? i : knn[(int64_t)i * K + tid - 1];
+    if (tid <= kc) s_fib[tid] = tid == 0 ? i : knn[(int64_t)i * kstride + tid - 1];
     __syncthreads();
-    // gather the cluster matrix (column-major in A: consecutive threads read
-    // consecutive rows of one column)
+    // gather S^T: sm[r][c] = S[c][r] = A(row of cluster index c, column of r);
+    // consecutive threads read consecutive rows of one column of A
     for (int idx = tid; idx < s * s; idx += nt) {
-        const int c = idx / s, r = idx - c * s;
-        const int64_t gr = (int64_t)s_fib[r / nb] * nb + r % nb;
-        const int64_t gc = (int64_t)s_fib[c / nb] * nb + c % nb;
+        const int r = idx / s, c = idx - r * s;
+        const int64_t gr = (int64_t)s_fib[c / nb] * nb + c % nb;
+        const int64_t gc = (int64_t)s_fib[r / nb] * nb + r % nb;
         sm[r * ld + c] = (float)A[gc * lda + gr];
     }
     for (int idx = tid; idx < s * nb; idx += nt) {
@@ -180,10 +194,10 @@ __global__ void __launch_bounds__(256) cluster_inverse_kernel(int M, int nb, con
         }
         __syncthreads();
     }
+    float *dst = out + (int64_t)i * kPair * nb * nb;
     if (bad) {
         if (tid == 0) atomicAdd(singular, 1);
-        for (int idx = tid; idx < nb * nb; idx += nt)
-            out[(int64_t)i * nb * nb + idx] = (idx / nb == idx % nb) ? 1.f : 0.f;
+        for (int idx = tid; idx < kPair * nb * nb; idx += nt) dst[idx] = 0.f;  // P = I for this fiber
         return;
     }
     // back substitution on the nb right-hand sides, column-oriented: x_k,
@@ -197,26 +211,22 @@ __global__ void __launch_bounds__(256) cluster_inverse_kernel(int M, int nb, con
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < nb * nb; idx += nt) {
-        const int a = idx / nb, b = idx - a * nb;
-        out[(int64_t)i * nb * nb + idx] = sm[a * ld + s + b];
+    // B_{i,m}[a][b] = (S^-1)[a][(m+1) nb + b] = X[(m+1) nb + b][a]
+    for (int idx = tid; idx < kPair * nb * nb; idx += nt) {
+        const int m = idx / (nb * nb), e = idx - m * nb * nb;
+        const int a = e / nb, b = e - a * nb;
+        dst[idx] = m < kp ? sm[((m + 1) * nb + b) * ld + s + a] : 0.f;
     }
 }
 
 // ------------------------------------------------------------------ features
 // Frame of fiber i: e3 = t_i, e1 = the direction to the nearest neighbour
-// with its t_i component removed, e2 = e3 x e1.  Per neighbour (nearest
-// first): its centre relative to x_i in that frame, and the six distinct
-// products u_a u_b of its orientation u in the frame (invariant under the
-// sign of u, like the inverse block itself).
-__global__ void features_kernel(int M, const double *__restrict__ pos, const double *__restrict__ ori,
-                                const int *__restrict__ knn, float *__restrict__ feat, float *__restrict__ rot) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
+// with its t_i component removed, e2 = e3 x e1 (rows of E).
+__device__ void fiber_frame(const double *__restrict__ pos, const double *__restrict__ ori, int i, int j0,
+                            double E[3][3]) {
     const double *xi = pos + 3 * i, *ti = ori + 3 * i;
-    double e3[3] = {ti[0], ti[1], ti[2]};
-    const int j0 = knn[(int64_t)i * kK];
-    double d1[3] = {pos[3 * j0] - xi[0], pos[3 * j0 + 1] - xi[1], pos[3 * j0 + 2] - xi[2]};
+    const double e3[3] = {ti[0], ti[1], ti[2]};
+    const double d1[3] = {pos[3 * j0] - xi[0], pos[3 * j0 + 1] - xi[1], pos[3 * j0 + 2] - xi[2]};
     double dot = d1[0] * e3[0] + d1[1] * e3[1] + d1[2] * e3[2];
     double e1[3] = {d1[0] - dot * e3[0], d1[1] - dot * e3[1], d1[2] - dot * e3[2]};
     double n1 = sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
@@ -230,20 +240,56 @@ __global__ void features_kernel(int M, const double *__restrict__ pos, const dou
     }
     for (int a = 0; a < 3; ++a) e1[a] /= n1;
     const double e2[3] = {e3[1] * e1[2] - e3[2] * e1[1], e3[2] * e1[0] - e3[0] * e1[2], e3[0] * e1[1] - e3[1] * e1[0]};
-    const double *E[3] = {e1, e2, e3};
-    for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) rot[(int64_t)i * 9 + r * 3 + c] = (float)E[r][c];
-    float *f = feat + (int64_t)i * kIn;
-    for (int n = 0; n < kK; ++n) {
-        const int j = knn[(int64_t)i * kK + n];
+    for (int c = 0; c < 3; ++c) {
+        E[0][c] = e1[c];
+        E[1][c] = e2[c];
+        E[2][c] = e3[c];
+    }
+}
+
+// Features of the pair (fiber i, neighbour m), one thread per pair: nine
+// floats per neighbour in fiber i's frame.  Slot 0 is neighbour m: its
+// relative centre, its orientation u with the canonical sign (u_z > 0, ties
+// broken by u_y then u_x; the sign goes to sign[]) and u squared; slots
+// 1..15 are the other neighbours, nearest first: relative centre and the six
+// products u_a u_b (the sign of their orientation does not change block m).
+__global__ void pair_features_kernel(int M, int kp, const double *__restrict__ pos, const double *__restrict__ ori,
+                                     const int *__restrict__ knn, float *__restrict__ feat,
+                                     float *__restrict__ sign, float *__restrict__ rot) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)M * kp) return;
+    const int i = (int)(t / kp), m = (int)(t - (int64_t)i * kp);
+    const int *nb = knn + (int64_t)i * kK;
+    double E[3][3];
+    fiber_frame(pos, ori, i, nb[0], E);
+    if (m == 0)
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) rot[(int64_t)i * 9 + r * 3 + c] = (float)E[r][c];
+    const double *xi = pos + 3 * i;
+    float *f = feat + t * kIn;
+    auto local = [&](int j, double dl[3], double ul[3]) {
         const double d[3] = {pos[3 * j] - xi[0], pos[3 * j + 1] - xi[1], pos[3 * j + 2] - xi[2]};
         const double *tj = ori + 3 * j;
-        double dl[3], ul[3];
         for (int r = 0; r < 3; ++r) {
             dl[r] = E[r][0] * d[0] + E[r][1] * d[1] + E[r][2] * d[2];
             ul[r] = E[r][0] * tj[0] + E[r][1] * tj[1] + E[r][2] * tj[2];
         }
-        float *g = f + n * 9;
+    };
+    double dl[3], ul[3];
+    local(nb[m], dl, ul);
+    const bool pos_sign = ul[2] > 0.0 || (ul[2] == 0.0 && (ul[1] > 0.0 || (ul[1] == 0.0 && ul[0] >= 0.0)));
+    const double s = pos_sign ? 1.0 : -1.0;
+    sign[t] = (float)s;
+    for (int r = 0; r < 3; ++r) {
+        f[r] = (float)dl[r];
+        f[3 + r] = (float)(s * ul[r]);
+        f[6 + r] = (float)(ul[r] * ul[r]);
+    }
+    int slot = 1;
+    for (int n = 0; n < kK; ++n) {
+        if (n == m) continue;
+        local(nb[n], dl, ul);
+        float *g = f + slot * 9;
         g[0] = (float)dl[0];
         g[1] = (float)dl[1];
         g[2] = (float)dl[2];
@@ -253,44 +299,50 @@ __global__ void features_kernel(int M, const double *__restrict__ pos, const dou
         g[6] = (float)(ul[0] * ul[1]);
         g[7] = (float)(ul[0] * ul[2]);
         g[8] = (float)(ul[1] * ul[2]);
+        ++slot;
     }
 }
 
-// local <-> global block transform: B = I + R_blk^T O R_blk (to_global) or
-// O = R_blk (B - I) R_blk^T (to_local), R_blk = I_5 (x) R, per fiber.
-__global__ void block_frame_kernel(int M, const float *__restrict__ rot, const float *__restrict__ in,
-                                   float *__restrict__ out, int to_global) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
+// local <-> global pair blocks: B = (R_blk^T O R_blk) D (to_global) or
+// O = (R_blk B R_blk^T) D (to_local), R_blk = I_5 (x) R of fiber i, D = the
+// pair's sign on the columns of odd Legendre order k (lb = k - 1 even).  One
+// thread per pair block; the output of pairs m >= kp is zero.
+__global__ void pair_frame_kernel(int M, int kp, const float *__restrict__ rot, const float *__restrict__ sign,
+                                  const float *__restrict__ in, int64_t in_stride, float *__restrict__ out,
+                                  int64_t out_stride, int to_global) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)M * kPair) return;
+    const int i = (int)(t / kPair), m = (int)(t - (int64_t)i * kPair);
+    const int64_t q = (int64_t)i * kp + m;  // row of the per-pair arrays (features, MLP output)
+    float *Y = out + (to_global ? t : q) * out_stride;
+    if (m >= kp) {
+        if (to_global)
+            for (int e = 0; e < kOut; ++e) Y[e] = 0.f;
+        return;
+    }
     float R[9];
-    for (int t = 0; t < 9; ++t) R[t] = rot[(int64_t)i * 9 + t];
-    const float *X = in + (int64_t)i * kOut;
-    float *Y = out + (int64_t)i * kOut;
+    for (int e = 0; e < 9; ++e) R[e] = rot[(int64_t)i * 9 + e];
+    const float s = sign[q];
+    const float *X = in + (to_global ? q : t) * in_stride;
     for (int kb = 0; kb < 5; ++kb)
         for (int lb = 0; lb < 5; ++lb) {
-            float O[3][3], T[3][3], Z[3][3];
+            float O[3][3], T[3][3];
             for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b) {
-                    float v = X[(kb * 3 + a) * kNb + lb * 3 + b];
-                    if (!to_global && kb == lb && a == b) v -= 1.f;
-                    O[a][b] = v;
-                }
+                for (int b = 0; b < 3; ++b) O[a][b] = X[(kb * 3 + a) * kNb + lb * 3 + b];
             // to_global: Z = R^T O R ; to_local: Z = R O R^T
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) {
-                    float sacc = 0.f;
-                    for (int c = 0; c < 3; ++c) sacc += O[a][c] * (to_global ? R[c * 3 + b] : R[b * 3 + c]);
-                    T[a][b] = sacc;
+                    float acc = 0.f;
+                    for (int c = 0; c < 3; ++c) acc += O[a][c] * (to_global ? R[c * 3 + b] : R[b * 3 + c]);
+                    T[a][b] = acc;
                 }
+            const float d = (lb % 2 == 0) ? s : 1.f;
             for (int a = 0; a < 3; ++a)
                 for (int b = 0; b < 3; ++b) {
-                    float sacc = 0.f;
-                    for (int c = 0; c < 3; ++c) sacc += (to_global ? R[c * 3 + a] : R[a * 3 + c]) * T[c][b];
-                    Z[a][b] = sacc;
+                    float acc = 0.f;
+                    for (int c = 0; c < 3; ++c) acc += (to_global ? R[c * 3 + a] : R[a * 3 + c]) * T[c][b];
+                    Y[(kb * 3 + a) * kNb + lb * 3 + b] = d * acc;
                 }
-            for (int a = 0; a < 3; ++a)
-                for (int b = 0; b < 3; ++b)
-                    Y[(kb * 3 + a) * kNb + lb * 3 + b] = Z[a][b] + ((to_global && kb == lb && a == b) ? 1.f : 0.f);
         }
 }
 
@@ -440,6 +492,58 @@ cudaError_t mlp_forward(const float *W, int rows, const float *X, float *H1, flo
 }  // namespace
 
 // ------------------------------------------------------------------ handle side
+namespace {
+// neighbours found by knn_kernel (stride kK per fiber) and blocks kept per fiber
+int knn_count(const rf_handle *h) { return std::min(kK, h->M - 1); }
+
+rf_status ensure_pair_buffers(rf_handle *h) {
+    const int M = h->M, nb = 3 * h->N;
+    auto ck = [&](cudaError_t e, const char *what) -> rf_status {
+        return e == cudaSuccess ? RF_OK : cuda_fail(h, e, what);
+    };
+    rf_status s;
+    if (!h->Pblocks &&
+        (s = ck(cudaMalloc(&h->Pblocks, sizeof(float) * (size_t)M * kPair * nb * nb), "alloc blocks")) != RF_OK)
+        return s;
+    if (!h->knn && (s = ck(cudaMalloc(&h->knn, sizeof(int) * (size_t)M * kK), "alloc knn")) != RF_OK) return s;
+    return RF_OK;
+}
+
+rf_status ensure_mlp_buffers(rf_handle *h) {
+    const size_t rows = (size_t)h->M * kPair;
+    auto ck = [&](cudaError_t e, const char *what) -> rf_status {
+        return e == cudaSuccess ? RF_OK : cuda_fail(h, e, what);
+    };
+    rf_status s;
+    if (h->feat) return RF_OK;
+    // features, then the frames (9 per fiber) and the pair signs (1 per pair)
+    if ((s = ck(cudaMalloc(&h->feat, sizeof(float) * (rows * kIn + (size_t)h->M * 9 + rows)), "alloc")) != RF_OK)
+        return s;
+    if ((s = ck(cudaMalloc(&h->mlp_h1, sizeof(float) * rows * kHid), "alloc")) != RF_OK) return s;
+    if ((s = ck(cudaMalloc(&h->mlp_h2, sizeof(float) * rows * kHid), "alloc")) != RF_OK) return s;
+    if ((s = ck(cudaMalloc(&h->mlp_out, sizeof(float) * rows * kOut), "alloc")) != RF_OK) return s;
+    return RF_OK;
+}
+
+float *feat_rot(rf_handle *h) { return h->feat + (size_t)h->M * kPair * kIn; }
+float *feat_sign(rf_handle *h) { return feat_rot(h) + (size_t)h->M * 9; }
+
+cudaError_t launch_knn(rf_handle *h) {
+    knn_kernel<<<(h->M + kKnnWarps - 1) / kKnnWarps, kKnnWarps * 32, 0, h->stream>>>(h->M, h->X[h->cur], kK, h->knn);
+    h->launches++;
+    return cudaGetLastError();
+}
+
+// pair features (M x kPair rows), the frames and the signs of the current state
+cudaError_t launch_pair_features(rf_handle *h) {
+    const int64_t rows = (int64_t)h->M * kPair;
+    pair_features_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, h->stream>>>(
+        h->M, kPair, h->X[h->cur], h->T[h->cur], h->knn, h->feat, feat_sign(h), feat_rot(h));
+    h->launches++;
+    return cudaGetLastError();
+}
+}  // namespace
+
 rf_status build_preconditioner(rf_handle *h) {
     const int M = h->M, nb = 3 * h->N;
     cudaStream_t st = h->stream;
@@ -447,19 +551,13 @@ rf_status build_preconditioner(rf_handle *h) {
         return e == cudaSuccess ? RF_OK : cuda_fail(h, e, what);
     };
     rf_status s;
-    if (!h->Pblocks) {
-        if ((s = ck(cudaMalloc(&h->Pblocks, sizeof(float) * (size_t)M * nb * nb), "alloc blocks")) != RF_OK) return s;
-    }
-    const int kmax = kK;
-    if (!h->knn) {
-        if ((s = ck(cudaMalloc(&h->knn, sizeof(int) * (size_t)M * kmax), "alloc knn")) != RF_OK) return s;
-    }
-    const int K = std::min(kmax, M - 1);
-    knn_kernel<<<(M + kKnnWarps - 1) / kKnnWarps, kKnnWarps * 32, 0, st>>>(M, h->X[h->cur], K, h->knn);
-    h->launches++;
-    if ((s = ck(cudaGetLastError(), "knn")) != RF_OK) return s;
+    if ((s = ensure_pair_buffers(h)) != RF_OK) return s;
+    const int K = knn_count(h);
+    if ((s = ck(launch_knn(h), "knn")) != RF_OK) return s;
+    h->pc_pairs = 0;
     if (h->p.preconditioner == RF_PC_CLUSTER) {
-        const int kc = std::min(h->p.cluster_size, K);
+        const int kc = std::max(1, std::min(h->p.cluster_size, K));
+        const int kp = std::min(kPair, kc);
         const int sdim = (kc + 1) * nb;
         const size_t smem = sizeof(float) * (size_t)sdim * (sdim + nb + 1);
         if (smem > 227 * 1024)
@@ -469,22 +567,23 @@ rf_status build_preconditioner(rf_handle *h) {
         cudaMemsetAsync(sing, 0, sizeof(int), st);
         cudaError_t e;
         if (h->A64) {
-            e = cudaFuncSetAttribute(cluster_inverse_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(cluster_rows_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
             if (e == cudaSuccess)
-                cluster_inverse_kernel<double><<<M, 256, smem, st>>>(M, nb, h->A64, h->lda, h->knn, K, kc, h->Pblocks,
-                                                                     sing);
+                cluster_rows_kernel<double><<<M, 256, smem, st>>>(M, nb, h->A64, h->lda, h->knn, kK, kc, kp,
+                                                                  h->Pblocks, sing);
         } else {
-            e = cudaFuncSetAttribute(cluster_inverse_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            e = cudaFuncSetAttribute(cluster_rows_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
             if (e == cudaSuccess)
-                cluster_inverse_kernel<float><<<M, 256, smem, st>>>(M, nb, h->A32, h->lda, h->knn, K, kc, h->Pblocks,
-                                                                    sing);
+                cluster_rows_kernel<float><<<M, 256, smem, st>>>(M, nb, h->A32, h->lda, h->knn, kK, kc, kp,
+                                                                 h->Pblocks, sing);
         }
         h->launches++;
         if (e == cudaSuccess) e = cudaGetLastError();
         cudaFree(sing);
         if ((s = ck(e, "cluster inverse")) != RF_OK) return s;
+        h->pc_pairs = kp;
         h->pc_ready = true;
         return RF_OK;
     }
@@ -503,19 +602,15 @@ rf_status apply_mlp(rf_handle *h) {
         return e == cudaSuccess ? RF_OK : cuda_fail(h, e, what);
     };
     rf_status s;
-    if (!h->feat) {
-        if ((s = ck(cudaMalloc(&h->feat, sizeof(float) * ((size_t)M * (kIn + 9))), "alloc")) != RF_OK) return s;
-        if ((s = ck(cudaMalloc(&h->mlp_h1, sizeof(float) * (size_t)M * kHid), "alloc")) != RF_OK) return s;
-        if ((s = ck(cudaMalloc(&h->mlp_h2, sizeof(float) * (size_t)M * kHid), "alloc")) != RF_OK) return s;
-        if ((s = ck(cudaMalloc(&h->mlp_out, sizeof(float) * (size_t)M * kOut), "alloc")) != RF_OK) return s;
-    }
-    float *rot = h->feat + (size_t)M * kIn;
-    features_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, h->X[h->cur], h->T[h->cur], h->knn, h->feat, rot);
-    if ((s = ck(cudaGetLastError(), "features")) != RF_OK) return s;
-    if ((s = ck(mlp_forward(h->mlp_w, M, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out, st), "mlp")) != RF_OK) return s;
-    block_frame_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, rot, h->mlp_out, h->Pblocks, 1);
-    h->launches += 5;
+    if ((s = ensure_mlp_buffers(h)) != RF_OK) return s;
+    if ((s = ck(launch_pair_features(h), "features")) != RF_OK) return s;
+    const int rows = M * kPair;
+    if ((s = ck(mlp_forward(h->mlp_w, rows, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out, st), "mlp")) != RF_OK) return s;
+    pair_frame_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(M, kPair, feat_rot(h), feat_sign(h), h->mlp_out,
+                                                                       kOut, h->Pblocks, kOut, 1);
+    h->launches += 4;
     if ((s = ck(cudaGetLastError(), "block frame")) != RF_OK) return s;
+    h->pc_pairs = kPair;
     h->pc_ready = true;
     return RF_OK;
 }
@@ -560,21 +655,13 @@ rf_status rf_compute_features(rf_handle *h, float *features) {
     if (!h || !features) return fail(h, RF_ERR_INVALID_ARG, "null argument");
     if (h->M <= kK) return fail(h, RF_ERR_INVALID_ARG, "features need more than 16 fibers");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, RF_ERR_CUDA, "cudaSetDevice");
-    const int M = h->M;
-    if (!h->knn && cudaMalloc(&h->knn, sizeof(int) * (size_t)M * kK) != cudaSuccess) return fail(h, RF_ERR_OOM, "alloc");
-    if (!h->feat) {
-        if (cudaMalloc(&h->feat, sizeof(float) * ((size_t)M * (kIn + 9))) != cudaSuccess ||
-            cudaMalloc(&h->mlp_h1, sizeof(float) * (size_t)M * kHid) != cudaSuccess ||
-            cudaMalloc(&h->mlp_h2, sizeof(float) * (size_t)M * kHid) != cudaSuccess ||
-            cudaMalloc(&h->mlp_out, sizeof(float) * (size_t)M * kOut) != cudaSuccess)
-            return fail(h, RF_ERR_OOM, "alloc");
-    }
-    knn_kernel<<<(M + kKnnWarps - 1) / kKnnWarps, kKnnWarps * 32, 0, h->stream>>>(M, h->X[h->cur], kK, h->knn);
-    features_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->X[h->cur], h->T[h->cur], h->knn, h->feat,
-                                                            h->feat + (size_t)M * kIn);
-    h->launches += 2;
-    cudaError_t e = cudaMemcpyAsync(features, h->feat, sizeof(float) * (size_t)M * kIn, cudaMemcpyDeviceToHost,
-                                    h->stream);
+    rf_status s;
+    if ((s = ensure_pair_buffers(h)) != RF_OK || (s = ensure_mlp_buffers(h)) != RF_OK) return s;
+    cudaError_t e = launch_knn(h);
+    if (e == cudaSuccess) e = launch_pair_features(h);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(features, h->feat, sizeof(float) * (size_t)h->M * kPair * kIn, cudaMemcpyDeviceToHost,
+                            h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "features");
     return RF_OK;
@@ -585,21 +672,25 @@ rf_status rf_compute_cluster_targets(rf_handle *h, float *targets) {
     if (!h->assembled) return fail(h, RF_ERR_INVALID_ARG, "cluster targets need an assembled system");
     if (3 * h->N != kNb) return fail(h, RF_ERR_INVALID_ARG, "the learned blocks are built for N = 5");
     if (h->M <= kK) return fail(h, RF_ERR_INVALID_ARG, "targets need more than 16 fibers");
+    if (h->p.cluster_size < kPair) return fail(h, RF_ERR_INVALID_ARG, "targets need cluster_size >= 8");
     if (cudaSetDevice(h->device) != cudaSuccess) return fail(h, RF_ERR_CUDA, "cudaSetDevice");
     const int saved = h->p.preconditioner;
     h->p.preconditioner = RF_PC_CLUSTER;
-    rf_status s = build_preconditioner(h);   // exact blocks into Pblocks
+    rf_status s = build_preconditioner(h);   // exact coupling blocks into Pblocks
     h->p.preconditioner = saved;
     if (s != RF_OK) return s;
-    const int M = h->M;
-    // features (frames) of the same state, then the blocks in that frame minus I
-    std::vector<float> tmp((size_t)M * kIn);
-    s = rf_compute_features(h, tmp.data());
-    if (s != RF_OK) return s;
-    block_frame_kernel<<<(M + 127) / 128, 128, 0, h->stream>>>(M, h->feat + (size_t)M * kIn, h->Pblocks, h->mlp_out, 0);
-    h->launches++;
-    cudaError_t e = cudaMemcpyAsync(targets, h->mlp_out, sizeof(float) * (size_t)M * kOut, cudaMemcpyDeviceToHost,
-                                    h->stream);
+    // the frames and signs of the same state, then the blocks in that frame
+    if ((s = ensure_mlp_buffers(h)) != RF_OK) return s;
+    const int64_t rows = (int64_t)h->M * kPair;
+    cudaError_t e = launch_pair_features(h);
+    if (e == cudaSuccess) {
+        pair_frame_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, h->stream>>>(
+            h->M, kPair, feat_rot(h), feat_sign(h), h->Pblocks, kOut, h->mlp_out, kOut, 0);
+        h->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(targets, h->mlp_out, sizeof(float) * rows * kOut, cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "targets");
     if (saved != RF_PC_CLUSTER) h->pc_ready = false;

@@ -118,9 +118,11 @@ cudaError_t launch_normalize(int M, double *T, cudaStream_t st);
 // y[0:m) = A[0:m, 0:k) x, A column-major with leading dimension lda.
 // S storage type, X vector type, ACC accumulation type, Y output type.
 // mode 0: y = A x;  mode 1: y = r - A x (residual, r given)
+// stop (optional, device): when *stop != 0 at launch time every CTA returns at
+// once (a product queued ahead for a solve that has finished meanwhile).
 template <typename S, typename X, typename ACC, typename Y>
 cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *x, Y *y, const Y *r,
-                        ACC *work, int64_t work_elems, int sm_count, cudaStream_t st);
+                        ACC *work, int64_t work_elems, int sm_count, cudaStream_t st, const int *stop = nullptr);
 int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes);
 
 // ---- Krylov vector kernels ----------------------------------------------------
@@ -179,9 +181,57 @@ template <typename T>
 cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols, double *out,
                                cudaStream_t st);
 
-// ---- block-diagonal preconditioner (15x15 blocks per fiber, FP32) -------------
-// z = blockdiag(B) v, B[i] row-major 3N x 3N
+// ---- neighbour-block preconditioner (FP32 blocks) -----------------------------
+// z_i = v_i + sum_{m < kp} B[i][m] v_{knn[i][m]}, B[i][m] row-major 3N x 3N,
+// pstride blocks per fiber, kstride neighbours per fiber in knn
 template <typename T>
-cudaError_t launch_block_apply(int M, int nb, const float *B, const T *v, T *z, cudaStream_t st);
+cudaError_t launch_pair_apply(int M, int nb, int kp, int pstride, const float *B, const int *knn, int kstride,
+                              const T *v, T *z, cudaStream_t st, const int *stop = nullptr);
+
+// ---- device-controlled Arnoldi steps (arnoldi.cu) -------------------------------
+// State of one GMRES(m) solve held on the device: the Hessenberg columns after
+// the Givens rotations, the rotations, the rotated right-hand side g, the
+// least-squares solution y, the Gram-Schmidt coefficients of the running step.
+constexpr int kArnoldiMax = 16;   // longest restart the device-controlled solve takes
+struct ArnoldiCtrl {
+    double H[kArnoldiMax * kArnoldiMax];   // H[r + c * kArnoldiMax], r <= c (upper triangle after rotation)
+    double g[kArnoldiMax + 1];
+    double cs[kArnoldiMax], sn[kArnoldiMax];
+    double y[kArnoldiMax];
+    double h1[kArnoldiMax], h2[kArnoldiMax];   // the two Gram-Schmidt passes of the running step
+    double hnext;      // norm of the new basis vector before normalisation
+    double bn;         // norm of the solve's right-hand side
+    double tol;        // stop when |g_k| / bn <= tol
+    double bea;        // the Arnoldi estimate |g_k| / bn after the last step
+    int k;             // Arnoldi steps of the current cycle
+    int itn;           // steps over all cycles
+    int iter_max;      // step budget
+    int stop;          // 0 running, 1 estimate <= tol, 2 budget spent, 3 non-finite value
+};
+// One step's outcome as the host sees it (host-mapped memory written by the device).
+struct ArnoldiStat {
+    int stop;
+    int itn;
+    double bea;
+};
+// Start of a cycle: beta = |r| (r the cycle's residual); g = (beta, 0, ...),
+// k = 0, stop = 0 (1 if beta = 0, 3 if not finite), written to *stat
+// (host-mapped) too; with first != 0 also bn = beta, itn = 0 and the
+// tolerance and budget; then V_0 = r / beta.
+template <typename T>
+cudaError_t launch_arnoldi_start(int64_t n, const T *r, T *V0, ArnoldiCtrl *c, double tol, int iter_max, int first,
+                                 double *part, unsigned int *counter, int max_blocks, ArnoldiStat *stat,
+                                 cudaStream_t st);
+// Step j after w = A z: two classical Gram-Schmidt passes against V_0..V_j
+// (dots; update and dots; update and norm), then the Givens update of column
+// j, the stop test, the step's outcome into stat[j] (host-mapped), and
+// V_{j+1} = w / |w| unless the solve stopped or j + 1 = m.  Every kernel
+// returns at once when the solve has stopped before it.
+template <typename T>
+cudaError_t launch_arnoldi_orthogonalize(int64_t n, T *w, T *V, int j, int m, ArnoldiCtrl *c, ArnoldiStat *stat,
+                                         double *part, unsigned int *counter, int max_blocks, cudaStream_t st);
+// End of a cycle: y = H(0:k, 0:k)^-1 g(0:k) and u = V(:, 0:k) y.
+template <typename T>
+cudaError_t launch_arnoldi_combine(int64_t n, const T *V, ArnoldiCtrl *c, T *u, cudaStream_t st);
 
 }  // namespace rf

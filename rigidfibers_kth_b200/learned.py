@@ -1,12 +1,14 @@
-"""Learned block preconditioner: data generation and GPU training.
+"""Learned neighbour-block preconditioner: data generation and GPU training.
 
-Samples are (features, target) pairs of single fibers: the geometry of the
-16 nearest neighbours in the fiber's own frame (144 floats) and the exact
-block of the inverse of its k-NN cluster submatrix, minus the identity, in
-the same frame (225 floats).  Both come from the solver itself
-(rf_compute_features, rf_compute_cluster_targets) on seeded clouds.  The MLP
-(144 -> 256 -> 256 -> 225, ReLU) is trained on the GPU by the library's own
-forward/backward kernels and Adam (rf_trainer_*).
+Samples are (features, target) pairs of (fiber, neighbour) couplings: the
+geometry of the fiber's 16 nearest neighbours in its own frame, the
+neighbour whose block is predicted listed first (144 floats), and the
+coupling block of the inverse of the fiber's k-NN cluster submatrix for that
+neighbour in the same frame and sign convention (225 floats).  Both come
+from the solver itself (rf_compute_features, rf_compute_cluster_targets) on
+seeded clouds, 8 pairs per fiber.  The MLP (144 -> 256 -> 256 -> 225, ReLU)
+is trained on the GPU by the library's own forward/backward kernels and
+Adam (rf_trainer_*).
 """
 import ctypes
 
@@ -74,8 +76,9 @@ class Trainer:
             pass
 
 
-def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=12, device=0):
-    """Features and exact cluster-inverse targets of one seeded Gaussian cloud."""
+def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=8, device=0):
+    """Pair features and exact cluster-inverse coupling blocks of one seeded
+    Gaussian cloud ((M * 8) rows each)."""
     pos, ori = generate_layout(M, "gaussian", sigma, 0.2, seed=seed)
     p = FiberParams(slenderness=eps, device=device, cluster_size=cluster_size)
     with Simulation(Configuration(p, pos, ori)) as sim:
@@ -86,9 +89,10 @@ def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=12, device=0):
 
 
 def generate_dataset(n_samples, seed0=5000, m_range=(250, 2000), density_sigma4000=3.0, rng_seed=0, **kw):
-    """Seeded clouds of M in m_range with the density of the M=4000, sigma=3
-    cloud (sigma scaled by (M/4000)^(1/3), jittered by +-20 %); seeds start at
-    seed0 (disjoint from the evaluation seeds 1000-1999)."""
+    """n_samples pairs from seeded clouds of M in m_range with the density of
+    the M=4000, sigma=3 cloud (sigma scaled by (M/4000)^(1/3), jittered by
+    +-20 %); seeds start at seed0 (disjoint from the evaluation seeds
+    1000-1999)."""
     rng = np.random.default_rng(rng_seed)
     xs, ys, total, k = [], [], 0, 0
     while total < n_samples:

@@ -286,15 +286,18 @@ class Simulation:
         fp = ctypes.POINTER(ctypes.c_float)
         L.check(L.lib().rf_set_mlp_weights(self._h, w.ctypes.data_as(fp), w.size), self._h)
 
+    PAIRS = 8  # coupling blocks per fiber (RF_MLP_PAIRS)
+
     def features(self):
-        """k-NN features (M x 144) of the current state in each fiber's frame."""
-        f = np.zeros((self.M, 144), dtype=np.float32)
+        """Pair features ((M * 8) x 144, fiber-major) of the current state in each fiber's frame."""
+        f = np.zeros((self.M * self.PAIRS, 144), dtype=np.float32)
         L.check(L.lib().rf_compute_features(self._h, f.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), self._h)
         return f
 
     def cluster_targets(self):
-        """Exact cluster block inverses minus I, in each fiber's frame (M x 225); needs an assembled system."""
-        t = np.zeros((self.M, 225), dtype=np.float32)
+        """Exact coupling blocks of the local-cluster inverses ((M * 8) x 225), in
+        each fiber's frame with the neighbour's canonical sign; needs an assembled system."""
+        t = np.zeros((self.M * self.PAIRS, 225), dtype=np.float32)
         L.check(L.lib().rf_compute_cluster_targets(self._h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
                 self._h)
         return t

@@ -2,8 +2,9 @@
 
     python -m rigidfibers_kth_b200.train_preconditioner --out rigidfibers_kth_b200/mlp_weights.npy
 
-200k samples from seeded clouds (M = 250..2000, seeds from 5000), 30 epochs
-of minibatch Adam with the library's own forward/backward kernels.
+Pairs (fiber, one of its 8 nearest neighbours) from seeded clouds (M =
+250..2000, seeds from 5000), minibatch Adam with the library's own
+forward/backward kernels.
 """
 import argparse
 import json

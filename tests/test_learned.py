@@ -1,11 +1,12 @@
-"""Preconditioners: exact cluster blocks, the learned MLP, its GPU training.
+"""Preconditioners: exact neighbour coupling blocks, the learned MLP, its GPU training.
 
 * the numpy reference MLP (oracle/mlp_ref.py) against finite differences;
 * the GPU trainer's loss and gradient against that reference;
-* rotation invariance of the features and equivariance of the exact blocks;
+* rotation invariance of the pair features and equivariance of the exact
+  coupling blocks; their invariance under the sign of a fiber's orientation;
 * preconditioned solves reach the same FP64 answer;
-* a trained network beats the method without it (block-Jacobi = identity)
-  at predicting the exact blocks, and costs no iterations.
+* the exact coupling blocks and a trained network cut GMRES iterations
+  against the method without them (block-Jacobi = identity blocks).
 """
 import numpy as np
 import pytest
@@ -64,23 +65,53 @@ def test_features_and_targets_rotate_with_the_configuration():
             sim.assemble_system()
             out.append((sim.features(), sim.cluster_targets()))
     (f0, t0), (f1, t1) = out
+    assert f0.shape == (200 * 8, 144) and t0.shape == (200 * 8, 225)
     assert np.abs(f0 - f1).max() <= 1e-4 * np.abs(f0).max()
     assert np.abs(t0 - t1).max() <= 1e-3 * np.abs(t0).max()
 
 
 @pytest.mark.gpu
+def test_features_and_targets_ignore_the_sign_of_orientations():
+    """A fiber and the same fiber with its orientation reversed are one
+    physical object; the coefficients of odd Legendre order change sign with
+    the parameterisation.  The neighbours' canonical sign in the features and
+    the matching column signs of the targets make both independent of the
+    neighbours' orientation signs (the fiber's own sign changes its frame,
+    which the network sees)."""
+    pos, ori = rf.generate_layout(150, "gaussian", 1.1, 0.2, seed=1505)
+    flip = np.ones(150)
+    flip[::3] = -1.0
+    out = []
+    for T in (ori, ori * flip[:, None]):
+        with rf.Simulation(rf.Configuration(rf.FiberParams(slenderness=1e-3), pos, T)) as sim:
+            sim.assemble_system()
+            out.append((sim.features().reshape(150, 8, 144), sim.cluster_targets().reshape(150, 8, 225)))
+    (f0, t0), (f1, t1) = out
+    keep = flip > 0  # fibers whose own orientation (and frame) is unchanged
+    assert np.abs(f0[keep] - f1[keep]).max() <= 1e-5 * np.abs(f0).max()
+    assert np.abs(t0[keep] - t1[keep]).max() <= 1e-4 * np.abs(t0).max()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("M", [17, 700])
 def test_features_follow_the_nearest_neighbours(M):
-    """The first three features of neighbour r are its centre in the fiber's
-    frame: their norms are the 16 smallest centre distances, in order."""
+    """Slot 0 of pair (i, m) holds neighbour m's centre in fiber i's frame,
+    slots 1..15 the other neighbours nearest first: the norms are the 16
+    smallest centre distances in that order."""
     pos, ori = rf.generate_layout(M, "gaussian", 1.5 * (M / 200) ** (1 / 3), 0.2, seed=1510 + M)
     with rf.Simulation(rf.Configuration(rf.FiberParams(slenderness=1e-3), pos, ori)) as sim:
-        f = sim.features().reshape(M, 16, 9)
+        f = sim.features().reshape(M, 8, 16, 9)
     d = np.linalg.norm(pos[:, None, :] - pos[None, :, :], axis=-1)
     np.fill_diagonal(d, np.inf)
     want = np.sort(d, axis=1)[:, :16]
-    got = np.linalg.norm(f[:, :, :3], axis=-1)
-    assert np.abs(got - want).max() <= 1e-5 * want.max()
+    got = np.linalg.norm(f[..., :3], axis=-1)  # (M, 8, 16)
+    for m in range(8):
+        order = [m] + [n for n in range(16) if n != m]
+        assert np.abs(got[:, m] - want[:, order]).max() <= 1e-5 * want.max()
+    # slot 0: canonical orientation (u_z >= 0) and its squares
+    u = f[:, :, 0, 3:6]
+    assert (u[..., 2] >= 0).all()
+    assert np.abs(f[:, :, 0, 6:9] - u ** 2).max() <= 1e-6
 
 
 def _solve(pos, ori, pc, weights=None, prec=rf.PREC_FP64, tol=1e-10, max_iters=600):
@@ -103,33 +134,29 @@ def _residual_after(pos, ori, pc, weights=None, iters=10):
 
 
 @pytest.mark.gpu
-def test_cluster_preconditioner_same_answer_lower_residual():
+def test_cluster_preconditioner_same_answer_fewer_iterations():
     pos, ori = rf.generate_layout(800, "gaussian", 3.0 * (800 / 4000) ** (1 / 3), 0.2, seed=1600)
     x0, s0 = _solve(pos, ori, rf.PC_NONE)
     x1, s1 = _solve(pos, ori, rf.PC_CLUSTER)
     assert np.abs(x1 - x0).max() <= 1e-8 * np.abs(x0).max()
-    assert s1["iterations"] <= s0["iterations"], (s1, s0)
+    assert s1["iterations"] < s0["iterations"], (s1, s0)
     assert _residual_after(pos, ori, rf.PC_CLUSTER) < _residual_after(pos, ori, rf.PC_NONE)
 
 
 @pytest.mark.gpu
-def test_trained_network_beats_identity_blocks():
-    """Train on clouds with seeds disjoint from the evaluation cloud.  The
-    network's gain over the method without it (block-Jacobi, whose blocks are
-    the identity here) is measured on the held-out cloud: its blocks are much
-    closer to the exact cluster-inverse blocks than the identity is.  The
-    solve with the learned blocks reaches the same FP64 answer; on this
-    well-conditioned system (spectrum inside [0.5, 2]) no block-diagonal
-    preconditioner, exact or learned, cuts GMRES iterations, so the test only
-    checks that it costs none."""
+def test_trained_network_cuts_iterations():
+    """Train on clouds with seeds disjoint from the evaluation cloud.  On the
+    held-out cloud the network's coupling blocks are closer to the exact ones
+    than zero blocks (no preconditioning) are, and the preconditioned FP64
+    GMRES(10) reaches the same answer in fewer iterations than without."""
     from rigidfibers_kth_b200.learned import Trainer, cloud_samples, generate_dataset
 
-    X, Y = generate_dataset(20_000, seed0=7000, m_range=(300, 800))
+    X, Y = generate_dataset(100_000, seed0=7000, m_range=(300, 800))
     tr = Trainer(seed=11)
     tr.add_samples(X, Y)
-    first = tr.train(1, batch=256, lr=1e-3)
+    first = tr.train(1, batch=512, lr=1e-3)
     for _ in range(9):
-        last = tr.train(1, batch=256, lr=1e-3)
+        last = tr.train(1, batch=512, lr=1e-3)
     w = tr.weights()
     tr.close()
     assert last < first
@@ -138,13 +165,13 @@ def test_trained_network_beats_identity_blocks():
     Xh, Yh = cloud_samples(M, sigma, 1601)
     _, _, pred = mlp_ref.forward(w.astype(np.float64), Xh)
     mse_learned = float(np.mean((pred - Yh) ** 2))
-    mse_identity = float(np.mean(Yh.astype(np.float64) ** 2))
-    assert mse_learned < 0.8 * mse_identity, (mse_learned, mse_identity)
+    mse_zero = float(np.mean(Yh.astype(np.float64) ** 2))
+    assert mse_learned < 0.5 * mse_zero, (mse_learned, mse_zero)
     pos, ori = rf.generate_layout(M, "gaussian", sigma, 0.2, seed=1601)
     x0, s0 = _solve(pos, ori, rf.PC_NONE)
     x2, s2 = _solve(pos, ori, rf.PC_LEARNED, weights=w)
     assert np.abs(x2 - x0).max() <= 1e-8 * np.abs(x0).max()
-    assert s2["iterations"] <= s0["iterations"] + 1, (s2, s0)
+    assert s2["iterations"] < s0["iterations"], (s2, s0)
 
 
 @pytest.mark.gpu
