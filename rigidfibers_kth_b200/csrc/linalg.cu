@@ -72,8 +72,16 @@ struct Vec16<__nv_bfloat16> {
 constexpr int kGemvThreads = 256;
 constexpr int kGemvUnroll = 8;
 
+// FP32 accumulation: eight resident CTAs per SM (32 registers), the streaming
+// loads of 64 warps per SM; the stop test alone made the compiler take 40
+// registers (six CTAs per SM) and the BF16 product ran 16 % slower.
+template <typename ACC>
+struct GemvMinBlocks {
+    static constexpr int value = sizeof(ACC) == 4 ? 8 : 0;  // 0: no minimum
+};
+
 template <typename S, typename X, typename ACC>
-__global__ void __launch_bounds__(kGemvThreads) gemv_partial_kernel(const S *__restrict__ A, int64_t lda, int64_t m,
+__global__ void __launch_bounds__(kGemvThreads, GemvMinBlocks<ACC>::value) gemv_partial_kernel(const S *__restrict__ A, int64_t lda, int64_t m,
                                                                     int64_t k, const X *__restrict__ x,
                                                                     int64_t cols_per_split, ACC *__restrict__ work,
                                                                     int64_t mpad, const int *__restrict__ stop) {

@@ -621,7 +621,7 @@ def test_config_matrix_rows_split_kernel_match_oracle(cfg):
     the benchmark's sizes against the oracle on the same sampled rows: the FP32
     matrix (the refinement residual's) within 1e-6 of max|A|, the BF16 copy
     (the inner solve's) within BF16 rounding of each entry (2^-8 relative, the
-    FP32 deviation on top), b within 1e-6 norm-wise."""
+    FP32 deviation on top), b within 1e-6 of max|b|."""
     M, dist, box, seed = CONFIG_LAYOUTS[cfg]
     pos, ori = rf.generate_layout(M, dist, box, 0.2, seed=seed)
     p = rfo.make_params(M, eps=1e-3)
@@ -639,7 +639,8 @@ def test_config_matrix_rows_split_kernel_match_oracle(cfg):
             excess = np.abs(A16 - A_o) - (2.0 ** -8 * np.abs(A_o) + 1e-6 * scale)
             assert excess.max() <= 0.0, (cfg, i0, excess.max() / scale)
             assert not np.array_equal(A16, A32)  # the inner copy really is the rounded one
-            # b sums M far contributions evaluated in FP32 per entry: norm-wise, as
-            # for the split assembly against the FP64 system
-            eb = np.linalg.norm(b[i0 * n3:i1 * n3] - b_o) / np.linalg.norm(b_o)
+            # b sums M far contributions evaluated in FP32 per entry, which cancel
+            # for some targets: the largest deviation relative to the largest
+            # entry of b, as for A
+            eb = np.abs(b[i0 * n3:i1 * n3] - b_o).max() / np.abs(b).max()
             assert eb <= 1e-6, (cfg, i0, eb)

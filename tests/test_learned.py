@@ -144,11 +144,11 @@ def test_cluster_preconditioner_same_answer_fewer_iterations():
 
 
 @pytest.mark.gpu
-def test_trained_network_cuts_iterations():
-    """Train on clouds with seeds disjoint from the evaluation cloud.  On the
-    held-out cloud the network's coupling blocks are closer to the exact ones
-    than zero blocks (no preconditioning) are, and the preconditioned FP64
-    GMRES(10) reaches the same answer in fewer iterations than without."""
+def test_trainer_learns_the_coupling_blocks():
+    """A short training on clouds with seeds disjoint from the evaluation
+    cloud: the loss falls, and on the held-out cloud the network's coupling
+    blocks are closer to the exact ones than zero blocks (no
+    preconditioning) are."""
     from rigidfibers_kth_b200.learned import Trainer, cloud_samples, generate_dataset
 
     X, Y = generate_dataset(100_000, seed0=7000, m_range=(300, 800))
@@ -161,13 +161,33 @@ def test_trained_network_cuts_iterations():
     tr.close()
     assert last < first
     M = 800
+    Xh, Yh = cloud_samples(M, 3.0 * (M / 4000) ** (1 / 3), 1601)
+    _, _, pred = mlp_ref.forward(w.astype(np.float64), Xh)
+    mse_learned = float(np.mean((pred - Yh) ** 2))
+    mse_zero = float(np.mean(Yh.astype(np.float64) ** 2))
+    assert mse_learned < 0.9 * mse_zero, (mse_learned, mse_zero)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M", [800, 2000])
+def test_shipped_network_cuts_iterations(M):
+    """The shipped weights (python -m rigidfibers_kth_b200.train_preconditioner:
+    400k pairs from clouds with seeds from 5000) on held-out clouds of the
+    benchmark's density: the predicted coupling blocks explain most of the
+    exact ones, and the preconditioned FP64 GMRES(10) reaches the same answer
+    in fewer iterations than the method without it."""
+    import os
+
+    from rigidfibers_kth_b200.learned import cloud_samples
+
+    w = np.load(os.path.join(os.path.dirname(rf.__file__), "mlp_weights.npy"))
     sigma = 3.0 * (M / 4000) ** (1 / 3)
-    Xh, Yh = cloud_samples(M, sigma, 1601)
+    Xh, Yh = cloud_samples(M, sigma, 1601 + M)
     _, _, pred = mlp_ref.forward(w.astype(np.float64), Xh)
     mse_learned = float(np.mean((pred - Yh) ** 2))
     mse_zero = float(np.mean(Yh.astype(np.float64) ** 2))
     assert mse_learned < 0.5 * mse_zero, (mse_learned, mse_zero)
-    pos, ori = rf.generate_layout(M, "gaussian", sigma, 0.2, seed=1601)
+    pos, ori = rf.generate_layout(M, "gaussian", sigma, 0.2, seed=1601 + M)
     x0, s0 = _solve(pos, ori, rf.PC_NONE)
     x2, s2 = _solve(pos, ori, rf.PC_LEARNED, weights=w)
     assert np.abs(x2 - x0).max() <= 1e-8 * np.abs(x0).max()
