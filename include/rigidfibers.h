@@ -107,7 +107,13 @@ typedef struct rf_params {
                                             backward recursion reaches FP32 accuracy; raised to 10
                                             where the tile kernel runs: numeric integration, N > 5);
                                             >= 1e30 keeps every integral in FP64 */
-    int32_t reserved[8];
+    int32_t shard_index;                 /* row-block shard of this handle (0 .. shard_count - 1) */
+    int32_t shard_count;                 /* row-block shards (GPUs) the system is split over; 0 or 1: the
+                                            whole system.  A shard assembles the rows of its target fibers
+                                            (rf_shard_range) and keeps all state replicated; FP64,
+                                            GMRES, recomputed velocities, no block preconditioner.  Solve and
+                                            velocities need the shards' communicator (rf_create_sharded). */
+    int32_t reserved[6];
 } rf_params;
 
 /* GMRES / refinement statistics of the last solve. */
@@ -132,6 +138,24 @@ void rf_params_default(rf_params *p);
 rf_status rf_create(const rf_params *p, const double *positions, const double *orientations,
                     rf_handle **out);
 rf_status rf_destroy(rf_handle *h);
+
+/* ---- Row-block sharding over GPUs (the reference runs on one device; no
+ * counterpart there).  The system's rows belong to target fibers: shard r of
+ * R assembles the rows of fibers [t0, t1) = [r M / R, (r + 1) M / R)
+ * (rf_shard_range) with no communication; state, Krylov vectors and GMRES
+ * control are replicated, and each product ends with one NCCL all-gather of
+ * the shards' row blocks (the right-hand side and the velocities likewise,
+ * once per step).  FP64 GMRES path only.  One process per GPU: rank 0 makes
+ * an id with rf_shard_unique_id and sends it to the others by its own means;
+ * every rank then calls rf_create_sharded with the same id and
+ * p->shard_index = its rank, p->shard_count = the ranks (collective; NCCL is
+ * loaded at run time).  rf_create with shard_count > 1 makes a shard without
+ * a communicator: it assembles and returns its rows (rf_get_matrix_rows; the
+ * right-hand side's other rows stay zero) but cannot solve. */
+rf_status rf_shard_unique_id(uint8_t *nccl_id /* 128 bytes */);
+rf_status rf_shard_range(int32_t M, int32_t shard_count, int32_t shard_index, int32_t *t0, int32_t *t1);
+rf_status rf_create_sharded(const rf_params *p, const double *positions, const double *orientations,
+                            const uint8_t *nccl_id, rf_handle **out);
 
 /* Simulation::step: assemble, solve, velocities, advect (Euler if
  * current_timestep == 0, else the second-order multistep), then rotate the

@@ -29,5 +29,7 @@ from .simulation import (  # noqa: F401
     parse_configuration_files,
     parse_layout_file,
     parse_parameter_file,
+    shard_range,
+    shard_unique_id,
     write_layout_file,
 )

@@ -59,7 +59,9 @@ class RfParams(ctypes.Structure):
         ("cluster_size", ctypes.c_int32),
         ("inner_tol", ctypes.c_double),
         ("near_field_c", ctypes.c_double),
-        ("reserved", ctypes.c_int32 * 8),
+        ("shard_index", ctypes.c_int32),
+        ("shard_count", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -108,6 +110,10 @@ def lib():
         "rf_params_default": (None, [P]),
         "rf_create": (ctypes.c_int, [P, _dp, _dp, ctypes.POINTER(_h)]),
         "rf_destroy": (ctypes.c_int, [_h]),
+        "rf_create_sharded": (ctypes.c_int, [P, _dp, _dp, ctypes.c_char_p, ctypes.POINTER(_h)]),
+        "rf_shard_unique_id": (ctypes.c_int, [ctypes.c_char_p]),
+        "rf_shard_range": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
         "rf_step": (ctypes.c_int, [_h, ctypes.c_size_t]),
         "rf_assemble_system": (ctypes.c_int, [_h]),
         "rf_solve_system": (ctypes.c_int, [_h]),

@@ -23,6 +23,7 @@ cudaError_t dalloc(T **p, size_t count) {
 }
 
 void free_all(rf_handle *h) {
+    rf::shard_detach(h);
     for (int i = 0; i < 3; ++i) {
         cudaFree(h->X[i]);
         cudaFree(h->T[i]);
@@ -265,6 +266,16 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "use_direct_solver needs precision RF_PREC_FP64");
     if (p->gmres_restart < 1 || p->gmres_restart > 64 || !(p->gmres_tol > 0.0))
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "gmres_restart must be 1..64 and gmres_tol > 0");
+    const int shards = p->shard_count > 1 ? p->shard_count : 1;
+    if (shards > 1) {
+        if (shards > M || p->shard_index < 0 || p->shard_index >= shards)
+            return rf::fail(nullptr, RF_ERR_INVALID_ARG, "need shard_count <= num_fibers and 0 <= shard_index < shard_count");
+        if (p->precision != RF_PREC_FP64 || p->use_direct_solver || p->velocity_mode != RF_VEL_RECOMPUTE ||
+            p->preconditioner != RF_PC_NONE)
+            return rf::fail(nullptr, RF_ERR_INVALID_ARG,
+                            "row-block shards take the FP64 GMRES path with recomputed velocities and no block "
+                            "preconditioner");
+    }
     if (!finite_all(positions, 3 * (size_t)M) || !finite_all(orientations, 3 * (size_t)M))
         return rf::fail(nullptr, RF_ERR_NAN, "non-finite position or orientation");
     for (int i = 0; i < M; ++i) {
@@ -286,7 +297,12 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
     h->N = N;
     h->LQ = 3 * NoQI;
     h->n = 3LL * N * M;
-    h->lda = round_up(h->n, 64);
+    h->shards = shards;
+    h->shard = shards > 1 ? p->shard_index : 0;
+    rf::shard_range(M, shards, h->shard, &h->t0, &h->t1);
+    h->tpad = rf::shard_pad(M, shards);
+    h->n_loc = 3LL * N * (h->t1 - h->t0);
+    h->lda = round_up(h->n_loc, 64);   // the stored rows: this shard's (all of them unsharded)
     h->ldp = round_up(3LL * M, 64);
     h->device = p->device;
     auto bail = [&](cudaError_t err, const char *what) {
@@ -336,7 +352,7 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
         }
     }
     // assembly chunking: about 8 CTAs per SM in the grid
-    const int tiles = (M + 7) / 8;
+    const int tiles = (h->t1 - h->t0 + 7) / 8;
     int chunks = std::max(1, std::min(M, (h->sm_count * 8 + tiles - 1) / tiles));
     h->asm_chunk = (M + chunks - 1) / chunks;
     h->asm_chunks = (M + h->asm_chunk - 1) / h->asm_chunk;
@@ -346,7 +362,7 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
     CKC(dalloc(&h->x, h->n), "alloc x");
     CKC(cudaMemset(h->x, 0, h->n * 8), "memset x");
     CKC(cudaMemset(h->b, 0, h->n * 8), "memset b");
-    CKC(dalloc(&h->bpart, (size_t)h->asm_chunks * h->n), "alloc rhs partials");
+    CKC(dalloc(&h->bpart, (size_t)h->asm_chunks * h->n_loc), "alloc rhs partials");
     // the split assembly (FP32 far pairs, FP64 near pairs) for the reduced
     // precisions with analytic integration; near_field_c >= 1e30 asks for FP64
     // integrals everywhere and keeps the tile kernel
@@ -425,6 +441,22 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
     return RF_OK;
 }
 
+rf_status rf_create_sharded(const rf_params *p, const double *positions, const double *orientations,
+                            const uint8_t *nccl_id, rf_handle **out) {
+    if (!out || !p || !nccl_id) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "null argument");
+    rf_status s = rf_create(p, positions, orientations, out);
+    if (s != RF_OK) return s;
+    rf_handle *h = *out;
+    h->shards = p->shard_count > 1 ? p->shard_count : 1;   // one shard: a communicator of one rank
+    s = rf::shard_attach(h, nccl_id);
+    if (s != RF_OK) {
+        g_create_error = h->err;
+        rf_destroy(h);
+        *out = nullptr;
+    }
+    return s;
+}
+
 rf_status rf_destroy(rf_handle *h) {
     if (!h) return RF_ERR_INVALID_ARG;
     cudaSetDevice(h->device);
@@ -459,7 +491,9 @@ rf_status rf_assemble_system(rf_handle *h) {
     a.M = h->M;
     a.N = h->N;
     a.LQ = h->LQ;
-    a.n = h->n;
+    a.t0 = h->t0;
+    a.t1 = h->t1;
+    a.n = h->n_loc;
     a.pos = h->X[h->cur];
     a.ori = h->T[h->cur];
     a.tab = h->tab;
@@ -563,7 +597,10 @@ rf_status rf_assemble_system(rf_handle *h) {
                                                                                               : rf::kPModeMixed;
         CK(h, rf::launch_assemble(a, h->p.use_analytical_integration == 0, pmode, h->asm_chunks, h->stream),
            "assemble kernel");
-        CK(h, rf::launch_reduce_chunks(h->bpart, h->asm_chunks, h->n, h->n, h->b, h->stream), "rhs reduction");
+        CK(h, rf::launch_reduce_chunks(h->bpart, h->asm_chunks, h->n_loc, h->n_loc, h->b + 3LL * h->N * h->t0,
+                                       h->stream),
+           "rhs reduction");
+        if (h->comm) CK(h, rf::shard_allgather(h, h->b, 3 * h->N, nullptr), "right-hand side exchange");
         h->vpart_chunks = h->asm_chunks;
         h->launches += 2;
     }
@@ -645,8 +682,19 @@ rf_status rf_solve_system(rf_handle *h) {
             return rf::fail(h, RF_ERR_NOT_CONVERGED, msg);
         }
     } else if (prec == RF_PREC_FP64) {
+        if (h->shards > 1 && !h->comm)
+            return rf::fail(h, RF_ERR_INVALID_ARG, "a row-block shard solves with its communicator (rf_create_sharded)");
         rf::Gmres<double>::Op A = [h](const double *in, double *out) {
             h->launches += 2;
+            if (h->comm) {
+                // this shard's rows, then the row blocks of every shard
+                cudaError_t e = timed_product(h, 8.0 * h->lda * h->n, [&] {
+                    return rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n_loc, h->n, in,
+                                                                            h->shard_send, nullptr, h->work64,
+                                                                            h->work_elems, h->sm_count, h->stream);
+                });
+                return e == cudaSuccess ? rf::shard_allgather(h, out, 3 * h->N, h->shard_send) : e;
+            }
             return timed_product(h, 8.0 * h->lda * h->n, [&] {
                 return rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, in, out, nullptr,
                                                                        h->work64, h->work_elems, h->sm_count,
@@ -851,6 +899,8 @@ rf_status rf_update_velocities(rf_handle *h) {
     } else {
         rf::VelArgs a{};
         a.M = h->M;
+        a.t0 = h->t0;
+        a.t1 = h->t1;
         a.N = h->N;
         a.LQ = h->LQ;
         a.pos = h->X[h->cur];
@@ -860,8 +910,13 @@ rf_status rf_update_velocities(rf_handle *h) {
         a.part = h->velpart;
         a.chunk = h->vel_chunk;
         CK(h, rf::launch_velocity(a, h->p.use_analytical_integration == 0, h->vel_chunks, st), "velocity kernel");
-        CK(h, rf::launch_velocity_finish(h->M, h->T[h->cur], h->tab, h->velpart, h->vel_chunks, V, W, st),
+        CK(h, rf::launch_velocity_finish(h->M, h->t0, h->t1, h->T[h->cur], h->tab, h->velpart, h->vel_chunks, V, W,
+                                         st),
            "velocity finish");
+        if (h->comm) {
+            CK(h, rf::shard_allgather(h, V, 3, nullptr), "velocity exchange");
+            CK(h, rf::shard_allgather(h, W, 3, nullptr), "velocity exchange");
+        }
         h->launches += 2;
     }
     CK(h, cudaStreamSynchronize(st), "velocities");
@@ -942,6 +997,7 @@ rf_status rf_get_rhs(rf_handle *h, double *b) {
 
 rf_status rf_get_matrix(rf_handle *h, double *A) {
     if (!h || !A) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    if (h->shards > 1) return rf::fail(h, RF_ERR_INVALID_ARG, "a row-block shard holds its rows only: rf_get_matrix_rows");
     CK(h, cudaSetDevice(h->device), "cudaSetDevice");
     const int64_t n = h->n;
     double *col = nullptr;
@@ -964,9 +1020,12 @@ rf_status rf_get_matrix(rf_handle *h, double *A) {
 rf_status rf_get_matrix_rows(rf_handle *h, int32_t which, int64_t row0, int64_t rows, double *out) {
     if (!h || !out) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
     if (which != 0 && which != 1) return rf::fail(h, RF_ERR_INVALID_ARG, "which must be 0 or 1");
-    if (row0 < 0 || rows < 1 || row0 + rows > h->n) return rf::fail(h, RF_ERR_INVALID_ARG, "rows out of range");
+    const int64_t first = 3LL * h->N * h->t0;   // the stored rows are the system's rows [first, first + n_loc)
+    if (row0 < first || rows < 1 || row0 + rows > first + h->n_loc)
+        return rf::fail(h, RF_ERR_INVALID_ARG, "rows out of range (or outside this handle's row-block shard)");
     if (!h->assembled) return rf::fail(h, RF_ERR_INVALID_ARG, "no assembled system");
     CK(h, cudaSetDevice(h->device), "cudaSetDevice");
+    row0 -= first;
     double *dev = nullptr;
     const size_t bytes = sizeof(double) * (size_t)rows * (size_t)h->n;
     CK(h, cudaMalloc(&dev, bytes), "row block");
@@ -987,6 +1046,7 @@ rf_status rf_get_matrix_rows(rf_handle *h, int32_t which, int64_t row0, int64_t 
 
 rf_status rf_matvec(rf_handle *h, const double *x, double *y) {
     if (!h || !x || !y) return rf::fail(h, RF_ERR_INVALID_ARG, "null argument");
+    if (h->shards > 1) return rf::fail(h, RF_ERR_INVALID_ARG, "rf_matvec needs the whole system (not a row-block shard)");
     CK(h, cudaSetDevice(h->device), "cudaSetDevice");
     double *dx = nullptr, *dy = nullptr;
     CK(h, cudaMalloc(&dx, h->n * 8), "alloc");
@@ -1094,6 +1154,7 @@ double rf_timer_elapsed_ms(rf_handle *h, int32_t from, int32_t to) {
 
 rf_status rf_profile_matvec(rf_handle *h, int32_t reps, double *ms_per_product, double *bytes) {
     if (!h || reps < 1 || !ms_per_product) return rf::fail(h, RF_ERR_INVALID_ARG, "bad argument");
+    if (h->shards > 1) return rf::fail(h, RF_ERR_INVALID_ARG, "rf_profile_matvec needs the whole system");
     CK(h, cudaSetDevice(h->device), "cudaSetDevice");
     const int64_t n = h->n;
     void *xv = nullptr, *yv = nullptr;

@@ -79,12 +79,12 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
         s_wP[t] = w;
         if (m < NL) s_wPf[t] = (float)w;
     }
-    const int i0 = blockIdx.x * TI;
+    const int i0 = a.t0 + blockIdx.x * TI;   // first target of the tile (global index)
     for (int t = tid; t < TI * 3; t += nthreads) {
         const int ti = t / 3, c = t % 3;
         const int i = i0 + ti;
-        s_xt[t] = (i < a.M) ? a.pos[3 * i + c] : 0.0;
-        s_tt[t] = (i < a.M) ? a.ori[3 * i + c] : 1.0;
+        s_xt[t] = (i < a.t1) ? a.pos[3 * i + c] : 0.0;
+        s_tt[t] = (i < a.t1) ? a.ori[3 * i + c] : 1.0;
     }
     for (int t = tid; t < TI * NL * 6; t += nthreads) s_acc[t] = 0.0;
     __syncthreads();
@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
 
     const int j0 = blockIdx.y * a.chunk;
     const int j1 = min(a.M, j0 + a.chunk);
-    const int64_t row0 = (int64_t)i0 * 3 * N;
-    const int64_t rows_left = (int64_t)a.M * 3 * N - row0;
+    const int64_t row0 = (int64_t)(i0 - a.t0) * 3 * N;   // row of the stored matrix
+    const int64_t rows_left = (int64_t)(a.t1 - i0) * 3 * N;
     const int rows_valid = rows_left < (int64_t)RT ? (int)rows_left : RT;
 
     __shared__ int s_nlist;
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
         if (PMODE == kPModeFP64) {
             if (worker) {
                 double *g = s_G + (size_t)ti * NG * LDQ + qpos;
-                if (i < a.M && i != j) {
+                if (i < a.t1 && i != j) {
                     const double r0x = fsub(xbx, xs0), r0y = fsub(xby, xs1), r0z = fsub(xbz, xs2);
                     if (NUMERIC) {
                         double G[NL][6];
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
             if (worker) {
                 double *g = s_G + (size_t)ti * NG * LDQ + qpos;
                 bool need64 = false;
-                if (i < a.M && i != j) {
+                if (i < a.t1 && i != j) {
                     const double r0x = xbx - xs0, r0y = xby - xs1, r0z = xbz - xs2;
                     const double cq = r0x * r0x + r0y * r0y + r0z * r0z;
                     need64 = cq < a.near_c;
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
         const int gt = t / (3 * N + 6);
         const int r = t - gt * (3 * N + 6);
         const int ii = i0 + gt;
-        if (ii >= a.M) continue;
+        if (ii >= a.t1) continue;
         if (r >= 3 * N && !a.vpart) continue;
         const double *tt = s_tt + gt * 3;
         const double *f = tab.half_force;
@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
         if (r < 3 * N) {
             if (k == 1) v = -tab.D1 * tdc * tt[aa];
             else v = -tab.gamma[k] * (contr[aa] - tab.Ek[k] * tdc * tt[aa]);
-            a.bpart[(int64_t)blockIdx.y * a.n + (int64_t)ii * 3 * N + r] = v;
+            a.bpart[(int64_t)blockIdx.y * a.n + (int64_t)(ii - a.t0) * 3 * N + r] = v;
         } else {
             if (k == 0) v = 0.5 / tab.d * contr[aa];
             else v = 1.5 / tab.d * (contr[aa] - tdc * tt[aa]);
@@ -430,7 +430,7 @@ static cudaError_t launch_assemble_n(const AsmArgs &a, int nchunks, cudaStream_t
                               : assemble_kernel<N, NUMERIC, PMODE, TI * kMaxLQ, 2>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    dim3 grid((a.M + TI - 1) / TI, nchunks);
+    dim3 grid((a.t1 - a.t0 + TI - 1) / TI, nchunks);
     kern<<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
 }

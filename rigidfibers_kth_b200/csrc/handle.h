@@ -100,6 +100,16 @@ struct rf_handle {
         double bytes = 0.0;
     } gt;
 
+    // row-block shard (shard.cu): target fibers [t0, t1) of M; their rows
+    // n_loc = 3 N (t1 - t0) are the rows of the stored matrix (leading
+    // dimension lda); everything else is replicated
+    int shards = 1, shard = 0;
+    int t0 = 0, t1 = 0, tpad = 0;   // tpad: the largest shard's fibers
+    int64_t n_loc = 0;
+    void *comm = nullptr;           // ncclComm_t of the shards (rf_create_sharded)
+    double *shard_send = nullptr;   // 3 N tpad
+    double *shard_gather = nullptr; // shards x 3 N tpad
+
     rf_solve_stats stats{};
     int cold_solves = 0;  // mixed solves left that start from zero (poor warm start seen)
     bool assembled = false;
@@ -109,6 +119,14 @@ struct rf_handle {
 
 namespace rf {
 rf_status fail(rf_handle *h, rf_status s, const std::string &msg);
+// row-block shards (shard.cu)
+void shard_range(int M, int R, int r, int *t0, int *t1);
+int shard_pad(int M, int R);
+rf_status shard_attach(rf_handle *h, const uint8_t *nccl_id);
+void shard_detach(rf_handle *h);
+// gathers every shard's segment [unit t0, unit t1) of `full` into `full`;
+// send_ready: this shard's segment already in h->shard_send, or null
+cudaError_t shard_allgather(rf_handle *h, double *full, int unit, const double *send_ready);
 rf_status cuda_fail(rf_handle *h, cudaError_t e, const char *what);
 // preconditioner (precond.cu)
 rf_status build_preconditioner(rf_handle *h);

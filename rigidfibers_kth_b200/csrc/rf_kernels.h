@@ -17,7 +17,8 @@ constexpr int kPModeMixed = 1;  // FP32 far field, FP64 near field, FP32 project
 
 struct AsmArgs {
     int M, N, LQ;
-    int64_t n;                 // 3*N*M
+    int t0, t1;                // target fibers [t0, t1) (a row-block shard; 0, M for the whole system)
+    int64_t n;                 // rows of the stored matrix: 3*N*(t1 - t0); its row r is the system's row 3*N*t0 + r
     const double *pos, *ori;   // 3M each
     const Tables *tab;         // device tables
     double *A64;               // FP64 matrix or null
@@ -80,6 +81,7 @@ cudaError_t launch_reduce_chunks(const double *part, int nchunks, int64_t stride
 // ---- velocities (recompute path) -------------------------------------------
 struct VelArgs {
     int M, N, LQ;
+    int t0, t1;                // target fibers [t0, t1)
     const double *pos, *ori;
     const double *coeffs;      // n
     const Tables *tab;
@@ -100,8 +102,8 @@ struct MatfreeArgs {
 };
 cudaError_t launch_matfree(const MatfreeArgs &a, bool numeric, int nchunks, const double *x, double *y,
                            cudaStream_t st);
-// V = (local + 0.5*sum IF0)/d, W = 1.5/d (sum IF1 - (t.sum IF1) t)
-cudaError_t launch_velocity_finish(int M, const double *ori, const Tables *tab, const double *part,
+// V = (local + 0.5*sum IF0)/d, W = 1.5/d (sum IF1 - (t.sum IF1) t) for targets [t0, t1)
+cudaError_t launch_velocity_finish(int M, int t0, int t1, const double *ori, const Tables *tab, const double *part,
                                    int nchunks, double *V, double *W, cudaStream_t st);
 // reuse path: V = PV x + v0, W = PW x + w0 (+ local term)
 cudaError_t launch_velocity_reuse_finish(int M, const double *ori, const Tables *tab, const double *pv_x,

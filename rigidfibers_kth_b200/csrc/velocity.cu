@@ -38,12 +38,12 @@ __global__ void __launch_bounds__(TI * kMaxLQ) velocity_kernel(VelArgs a) {
         s_P[m * kMaxLQ + q] = tab.P[m][q];
     }
     __syncthreads();
-    const int i0 = blockIdx.x * TI;
+    const int i0 = a.t0 + blockIdx.x * TI;   // first target of the tile (global index)
     const int ti = tid / LQ, q = tid - ti * LQ;
     const int i = i0 + ti;
     const double sq = s_pv[q], wq = s_wv[q];
     double xb[3] = {0, 0, 0};
-    if (i < a.M) {
+    if (i < a.t1) {
         const double *xc = a.pos + 3 * i, *tc = a.ori + 3 * i;
         xb[0] = fadd(xc[0], fmul(sq, tc[0]));
         xb[1] = fadd(xc[1], fmul(sq, tc[1]));
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(TI * kMaxLQ) velocity_kernel(VelArgs a) {
     double if0[3] = {0, 0, 0}, if1[3] = {0, 0, 0};
     const int j0 = blockIdx.y * a.chunk;
     const int j1 = min(a.M, j0 + a.chunk);
-    if (i < a.M) {
+    if (i < a.t1) {
         for (int j = j0; j < j1; ++j) {
             if (j == i) continue;
             const double xs[3] = {__ldg(a.pos + 3 * j), __ldg(a.pos + 3 * j + 1), __ldg(a.pos + 3 * j + 2)};
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(TI * kMaxLQ) velocity_kernel(VelArgs a) {
     __syncthreads();
     for (int t = tid; t < TI * 6; t += nthreads) {
         const int gt = t / 6, c = t % 6;
-        if (i0 + gt >= a.M) continue;
+        if (i0 + gt >= a.t1) continue;
         double s = 0.0;
         for (int qq = 0; qq < LQ; ++qq) s += s_red[((size_t)gt * LQ + qq) * 6 + c];
         a.part[(int64_t)blockIdx.y * 6 * a.M + (int64_t)(i0 + gt) * 6 + c] = s;
@@ -127,7 +127,7 @@ static cudaError_t launch_velocity_n(const VelArgs &a, int nchunks, cudaStream_t
     auto kern = velocity_kernel<N, NUMERIC, TI>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return err;
-    dim3 grid((a.M + TI - 1) / TI, nchunks);
+    dim3 grid((a.t1 - a.t0 + TI - 1) / TI, nchunks);
     kern<<<grid, TI * a.LQ, smem, st>>>(a);
     return cudaGetLastError();
 }
@@ -152,11 +152,11 @@ cudaError_t launch_velocity(const VelArgs &a, bool numeric, int nchunks, cudaStr
 }
 
 // Local term and final scaling (coeffs_and_vels.f90:698-705, 723-730).
-__global__ void velocity_finish_kernel(int M, const double *ori, const Tables *tab, const double *part,
-                                       int nchunks, const double *pv_x, const double *pw_x, double *V,
-                                       double *W) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= M) return;
+__global__ void velocity_finish_kernel(int M, int t0, int t1, const double *ori, const Tables *tab,
+                                       const double *part, int nchunks, const double *pv_x, const double *pw_x,
+                                       double *V, double *W) {
+    const int i = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t1) return;
     const double d = tab->d, e = tab->e;
     const double *t = ori + 3 * i;
     const double *F = tab->force;
@@ -180,16 +180,17 @@ __global__ void velocity_finish_kernel(int M, const double *ori, const Tables *t
     }
 }
 
-cudaError_t launch_velocity_finish(int M, const double *ori, const Tables *tab, const double *part, int nchunks,
-                                   double *V, double *W, cudaStream_t st) {
-    velocity_finish_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, ori, tab, part, nchunks, nullptr, nullptr, V, W);
+cudaError_t launch_velocity_finish(int M, int t0, int t1, const double *ori, const Tables *tab, const double *part,
+                                   int nchunks, double *V, double *W, cudaStream_t st) {
+    velocity_finish_kernel<<<(t1 - t0 + 127) / 128, 128, 0, st>>>(M, t0, t1, ori, tab, part, nchunks, nullptr,
+                                                                   nullptr, V, W);
     return cudaGetLastError();
 }
 
 cudaError_t launch_velocity_reuse_finish(int M, const double *ori, const Tables *tab, const double *pv_x,
                                          const double *pw_x, const double *vpart, int nchunks, double *V,
                                          double *W, cudaStream_t st) {
-    velocity_finish_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, ori, tab, vpart, nchunks, pv_x, pw_x, V, W);
+    velocity_finish_kernel<<<(M + 127) / 128, 128, 0, st>>>(M, 0, M, ori, tab, vpart, nchunks, pv_x, pw_x, V, W);
     return cudaGetLastError();
 }
 

@@ -42,9 +42,11 @@ class FiberParams:
     velocity_mode: int = L.VEL_RECOMPUTE
     device: int = 0
     max_refinements: int = 30
-    cluster_size: int = 12
+    cluster_size: int = 8
     inner_tol: float = 1e-3
     near_field_c: float = 6.0
+    shard_index: int = 0
+    shard_count: int = 1
 
     def to_c(self):
         p = L.RfParams()
@@ -53,7 +55,7 @@ class FiberParams:
             "slenderness", "timestep", "num_fibers", "num_timesteps", "num_terms_in_force_expansion",
             "num_quadrature_intervals", "use_analytical_integration", "use_direct_solver", "gmres_restart",
             "gmres_max_iters", "gmres_tol", "precision", "preconditioner", "velocity_mode", "device",
-            "max_refinements", "cluster_size", "inner_tol", "near_field_c",
+            "max_refinements", "cluster_size", "inner_tol", "near_field_c", "shard_index", "shard_count",
         ):
             setattr(p, name, getattr(self, name))
         p.external_force[:] = list(self.external_force)
@@ -145,10 +147,29 @@ def min_segment_distance(positions, orientations):
     return L.lib().rf_min_segment_distance(len(pos) // 3, _ptr(pos), _ptr(ori))
 
 
-class Simulation:
-    """Simulation(Configuration) with the reference's step API, on the GPU."""
+def shard_range(M, shard_count, shard_index):
+    """Target fibers [t0, t1) of row-block shard `shard_index` of `shard_count`."""
+    t0, t1 = ctypes.c_int32(), ctypes.c_int32()
+    L.check(L.lib().rf_shard_range(M, shard_count, shard_index, ctypes.byref(t0), ctypes.byref(t1)))
+    return t0.value, t1.value
 
-    def __init__(self, configuration, **overrides):
+
+def shard_unique_id():
+    """A new NCCL id (128 bytes) for the shards' communicator; made on one rank
+    and sent to the others by the caller (e.g. torch.distributed)."""
+    buf = ctypes.create_string_buffer(128)
+    L.check(L.lib().rf_shard_unique_id(buf))
+    return buf.raw
+
+
+class Simulation:
+    """Simulation(Configuration) with the reference's step API, on the GPU.
+
+    With ``nccl_id`` (and the parameters' shard_index / shard_count) the
+    handle is one row-block shard of a system split over GPUs, one process
+    per GPU (rf_create_sharded: collective over the shards)."""
+
+    def __init__(self, configuration, nccl_id=None, **overrides):
         if isinstance(configuration, FiberParams):
             raise TypeError("Simulation takes a Configuration (parameters + layout)")
         params = configuration.parameters
@@ -163,7 +184,11 @@ class Simulation:
         self.n = 3 * self.N * self.M
         self._c = params.to_c()
         h = ctypes.c_void_p()
-        st = L.lib().rf_create(ctypes.byref(self._c), _ptr(pos), _ptr(ori), ctypes.byref(h))
+        if nccl_id is None:
+            st = L.lib().rf_create(ctypes.byref(self._c), _ptr(pos), _ptr(ori), ctypes.byref(h))
+        else:
+            assert len(nccl_id) == 128
+            st = L.lib().rf_create_sharded(ctypes.byref(self._c), _ptr(pos), _ptr(ori), bytes(nccl_id), ctypes.byref(h))
         L.check(st, None)
         self._h = h
         self.last_status = L.RF_OK
