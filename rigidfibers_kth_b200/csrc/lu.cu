@@ -14,8 +14,7 @@
 //                    over the whole GPU;
 //   lu_swap_kernel   the panel's row swaps applied to the trailing columns;
 //   lu_trsm_kernel   U12 = L11^-1 A12, one thread per trailing column;
-//   lu_gemm_kernel   A22 -= L21 U12, 64 x 64 tiles staged in shared memory,
-//                    products on the FP64 tensor cores (mma.sync m8n8k4).
+//   lu_gemm_kernel   A22 -= L21 U12, 64 x 64 tiles staged in shared memory.
 // The swaps are not applied to the L columns left of a panel: the forward
 // solve applies each panel's swaps to the right-hand side just before that
 // panel's columns of L, which is the same elimination (LINPACK's order).
@@ -193,20 +192,15 @@ __global__ void __launch_bounds__(128) lu_trsm_kernel(double *A, int64_t lda, in
         if (i < nb) col[i] = x[i];
 }
 
-// A22 -= L21 U12 over rows and columns [k + nb, n) on the FP64 tensor cores:
-// 64 x 64 tiles, 256 threads; the L21 and U12 tiles are staged in shared
-// memory, warp w computes rows 16 (w % 4) .. + 16 and columns 32 (w / 4) .. + 32
-// as 2 x 4 products of mma.sync m8n8k4 f64 over the nb = 32 panel columns (8
-// k-steps), then subtracts them from A22.  Operand fragments (m8n8k4, row.col):
-// A: thread holds A[lane / 4][lane % 4]; B: B[lane % 4][lane / 4]; C: rows
-// lane / 4, columns 2 (lane % 4) + {0, 1}.  Each product entry is a sum of 32
-// products, as in the FMA loop it replaces (summation order differs).
+// A22 -= L21 U12 over rows and columns [k + nb, n): 64 x 64 tiles, 256 threads,
+// 4 x 4 entries per thread (rows tx + 16 i, columns ty + 16 j: consecutive
+// threads touch consecutive rows of a column).
 __global__ void __launch_bounds__(256) lu_gemm_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb) {
-    __shared__ double s_a[kLuNb][64 + 1];  // L21 tile: [p][row]
+    __shared__ double s_a[kLuNb][64];      // L21 tile: [p][row]
     __shared__ double s_b[64][kLuNb + 1];  // U12 tile: [column][p]
     const int64_t base = k + nb;
     const int64_t r0 = base + blockIdx.x * 64, c0 = base + blockIdx.y * 64;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     for (int t = tid; t < kLuNb * 64; t += 256) {
         const int p = t / 64, r = t % 64;
         s_a[p][r] = (p < nb && r0 + r < n) ? A[(k + p) * lda + r0 + r] : 0.0;
@@ -214,39 +208,33 @@ __global__ void __launch_bounds__(256) lu_gemm_kernel(double *A, int64_t lda, in
         s_b[cc][q] = (q < nb && c0 + cc < n) ? A[(c0 + cc) * lda + k + q] : 0.0;
     }
     __syncthreads();
-    const int wr = 16 * (warp & 3), wc = 32 * (warp >> 2);
-    const int g = lane >> 2, t4 = lane & 3;
-    double acc[2][4][2];
+    double acc[4][4];
 #pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+#pragma unroll 8
+    for (int p = 0; p < kLuNb; ++p) {
+        double a[4], b[4];
 #pragma unroll
-    for (int ks = 0; ks < kLuNb / 4; ++ks) {
-        const int p = 4 * ks + t4;
-        double a[2], b[4];
+        for (int i = 0; i < 4; ++i) a[i] = s_a[p][tx + 16 * i];
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt) a[mt] = s_a[p][wr + 8 * mt + g];
+        for (int j = 0; j < 4; ++j) b[j] = s_b[ty + 16 * j][p];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) b[nt] = s_b[wc + 8 * nt + g][p];
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt)
-                dmma_8x8x4(acc[mt][nt][0], acc[mt][nt][1], a[mt], b[nt], acc[mt][nt][0], acc[mt][nt][1]);
+            for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
+    for (int j = 0; j < 4; ++j) {
+        const int64_t c = c0 + ty + 16 * j;
+        if (c >= n) continue;
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const int64_t c = c0 + wc + 8 * nt + 2 * t4 + e;
-            if (c >= n) continue;
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                const int64_t r = r0 + wr + 8 * mt + g;
-                if (r < n) A[c * lda + r] -= acc[mt][nt][e];
-            }
+        for (int i = 0; i < 4; ++i) {
+            const int64_t r = r0 + tx + 16 * i;
+            if (r < n) A[c * lda + r] -= acc[i][j];
         }
+    }
 }
 
 // Forward solve, panel k: the panel's swaps on x, then the unit lower
