@@ -149,7 +149,9 @@ rf_status rf_destroy(rf_handle *h);
  * an id with rf_shard_unique_id and sends it to the others by its own means;
  * every rank then calls rf_create_sharded with the same id and
  * p->shard_index = its rank, p->shard_count = the ranks (collective; NCCL is
- * loaded at run time).  rf_create with shard_count > 1 makes a shard without
+ * loaded at run time: the file named by RF_NCCL_LIBRARY, else a copy already
+ * in the process, else libnccl.so.2; a process that also uses PyTorch loads
+ * PyTorch first, so that its NCCL is the one in use).  rf_create with shard_count > 1 makes a shard without
  * a communicator: it assembles and returns its rows (rf_get_matrix_rows; the
  * right-hand side's other rows stay zero) but cannot solve. */
 rf_status rf_shard_unique_id(uint8_t *nccl_id /* 128 bytes */);
@@ -286,6 +288,13 @@ rf_status rf_compute_features(rf_handle *h, float *features);
  * row-major 15 x 15, same order as the features), in the frame and sign
  * convention of the MLP output: the training targets.  Needs cluster_size >= 8. */
 rf_status rf_compute_cluster_targets(rf_handle *h, float *targets);
+
+/* The network's inference as the preconditioner runs it (tensor cores:
+ * tcgen05 MMAs with BF16 operands and FP32 accumulation in tensor memory),
+ * on count feature rows (count x 144) with the given weights; out is
+ * count x 225.  For checking the inference against the FP32 reference
+ * network (no counterpart in the reference). */
+rf_status rf_mlp_predict(int32_t device, const float *weights, const float *features, int64_t count, float *out);
 
 /* Stand-alone trainer on the device: owns weights, Adam state and a dataset. */
 typedef struct rf_trainer rf_trainer;

@@ -150,6 +150,7 @@ def lib():
         "rf_set_mlp_weights": (ctypes.c_int, [_h, _fp, ctypes.c_int64]),
         "rf_compute_features": (ctypes.c_int, [_h, _fp]),
         "rf_compute_cluster_targets": (ctypes.c_int, [_h, _fp]),
+        "rf_mlp_predict": (ctypes.c_int, [ctypes.c_int32, _fp, _fp, ctypes.c_int64, _fp]),
         "rf_trainer_create": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(_h)]),
         "rf_trainer_destroy": (ctypes.c_int, [_h]),
         "rf_trainer_add_samples": (ctypes.c_int, [_h, _fp, _fp, ctypes.c_int64]),

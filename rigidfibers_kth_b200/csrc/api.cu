@@ -34,7 +34,7 @@ void free_all(rf_handle *h) {
     }
     void *ptrs[] = {h->tab, h->A64, h->LU, h->lu_r, h->lu_piv, h->lu_info, h->mfpart, h->A32, h->A16, h->b, h->x, h->bpart, h->velpart, h->PV64, h->PW64,
                     h->PV32, h->PW32, h->vpart, h->pvx, h->pwx, h->work64, h->work32, h->r64, h->r32,
-                    h->d32, h->x32, h->Pblocks, h->knn, h->mlp_w, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out,
+                    h->d32, h->x32, h->Pblocks, h->knn, h->mlp_w, h->mlp_wtc, h->mlp_err, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out,
                     h->dscal, h->rb.partials, h->rb.counter, h->near_bits, h->near_list, h->near_cnt,
                     h->far_contr, h->near_contr, h->near_pref, h->near_off, h->near_total, h->nearbuf};
     for (void *p : ptrs) cudaFree(p);
@@ -351,8 +351,10 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
             CKC(cudaMemset(h->A16, 0, asz * 2), "memset A");
         }
     }
-    // assembly chunking: about 8 CTAs per SM in the grid
-    const int tiles = (h->t1 - h->t0 + 7) / 8;
+    // assembly chunking: about 8 CTAs per SM in the grid (from the whole
+    // system's targets also for a row-block shard, so that its right-hand
+    // side sums the same source chunks in the same order)
+    const int tiles = (M + 7) / 8;
     int chunks = std::max(1, std::min(M, (h->sm_count * 8 + tiles - 1) / tiles));
     h->asm_chunk = (M + chunks - 1) / chunks;
     h->asm_chunks = (M + h->asm_chunk - 1) / h->asm_chunk;
@@ -609,6 +611,14 @@ rf_status rf_assemble_system(rf_handle *h) {
         if (s != RF_OK) return s;
     }
     CK(h, cudaStreamSynchronize(h->stream), "assembly");
+    if (h->mlp_err && h->pc_ready && h->p.preconditioner == RF_PC_LEARNED) {
+        int herr = 0;
+        CK(h, cudaMemcpy(&herr, h->mlp_err, sizeof(int), cudaMemcpyDeviceToHost), "preconditioner status");
+        if (herr) {
+            h->pc_ready = false;
+            return rf::fail(h, RF_ERR_DEVICE_TIMEOUT, "tensor-core MLP: an MMA wait timed out");
+        }
+    }
     h->assembled = true;
     return RF_OK;
 }

@@ -30,8 +30,10 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int KM = kArnoldiMax;
 
+// one element per thread: the passes are latency bound, more CTAs keep more
+// loads in flight
 inline int blocks_for(int64_t n, int max_blocks) {
-    int64_t b = (n + kThreads * 4 - 1) / (kThreads * 4);
+    int64_t b = (n + kThreads - 1) / kThreads;
     if (b > max_blocks) b = max_blocks;
     if (b < 1) b = 1;
     return (int)b;
@@ -68,9 +70,13 @@ __device__ bool block_partials(const double (&v)[CMAX], int cnt, double *part, u
     return last;
 }
 
-__device__ double sum_partials(const double *part, int k) {
+// the partials of value k summed by one warp (lane-strided over the blocks,
+// then a fixed shuffle tree: the same order every run); valid in every lane
+__device__ double warp_sum_partials(const double *part, int k, int lane) {
     double s = 0.0;
-    for (unsigned int b = 0; b < gridDim.x; ++b) s += __ldcg(part + (int64_t)k * gridDim.x + b);
+    for (unsigned int b = lane; b < gridDim.x; b += 32) s += __ldcg(part + (int64_t)k * gridDim.x + b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;
 }
 
@@ -104,8 +110,9 @@ __global__ void __launch_bounds__(kThreads) start_kernel(int64_t n, const T *__r
         const double x = (double)r[e];
         v[0] += x * x;
     }
-    if (block_partials<1>(v, 1, part, counter) && threadIdx.x == 0) {
-        const double beta = sqrt(sum_partials(part, 0));
+    if (block_partials<1>(v, 1, part, counter) && threadIdx.x < 32) {
+        const double beta = sqrt(warp_sum_partials(part, 0, threadIdx.x));
+        if (threadIdx.x != 0) return;
         if (first) {
             c->bn = beta;
             c->itn = 0;
@@ -153,7 +160,11 @@ __global__ void __launch_bounds__(kThreads) cgs_dots_kernel(int64_t n, const T *
             if (k < j1) acc[k] += (double)V[(int64_t)k * n + e] * we;
     }
     if (block_partials<KM>(acc, j1, part, counter)) {
-        if ((int)threadIdx.x < j1) c->h1[threadIdx.x] = sum_partials(part, threadIdx.x);
+        const int lane = threadIdx.x & 31;
+        for (int k = threadIdx.x >> 5; k < j1; k += kWarps) {
+            const double s = warp_sum_partials(part, k, lane);
+            if (lane == 0) c->h1[k] = s;
+        }
         if (threadIdx.x == 0) *counter = 0u;
     }
 }
@@ -187,7 +198,11 @@ __global__ void __launch_bounds__(kThreads) cgs_update_dots_kernel(int64_t n, T 
             if (k < j1) acc[k] += vk[k] * wr;
     }
     if (block_partials<KM>(acc, j1, part, counter)) {
-        if ((int)threadIdx.x < j1) c->h2[threadIdx.x] = sum_partials(part, threadIdx.x);
+        const int lane = threadIdx.x & 31;
+        for (int k = threadIdx.x >> 5; k < j1; k += kWarps) {
+            const double s = warp_sum_partials(part, k, lane);
+            if (lane == 0) c->h2[k] = s;
+        }
         if (threadIdx.x == 0) *counter = 0u;
     }
 }
@@ -216,8 +231,9 @@ __global__ void __launch_bounds__(kThreads) cgs_update_norm_kernel(int64_t n, T 
         const double wr = (double)ws;
         v[0] += wr * wr;
     }
-    if (block_partials<1>(v, 1, part, counter) && threadIdx.x == 0) {
-        const double hn = sqrt(sum_partials(part, 0));
+    if (block_partials<1>(v, 1, part, counter) && threadIdx.x < 32) {
+        const double hn = sqrt(warp_sum_partials(part, 0, threadIdx.x));
+        if (threadIdx.x != 0) return;
         double h[KM + 1];
         bool finite = isfinite(hn);
         for (int r = 0; r <= j; ++r) {

@@ -86,6 +86,8 @@ struct rf_handle {
     int pc_pairs = 0;          // coupling blocks in use per fiber
     int *knn = nullptr;        // M x RF_MLP_K neighbour lists, nearest first
     float *mlp_w = nullptr;    // MLP weights on the device
+    __nv_bfloat16 *mlp_wtc = nullptr;  // the three weight matrices in BF16, rows padded to 256 (tensor-core inference)
+    int *mlp_err = nullptr;    // set by the tensor-core layers when an MMA wait timed out
     bool mlp_loaded = false;
     float *feat = nullptr;     // (M x RF_MLP_PAIRS) x 144 pair features, M x 9 frames, M x RF_MLP_PAIRS signs
     float *mlp_h1 = nullptr, *mlp_h2 = nullptr, *mlp_out = nullptr;
@@ -119,6 +121,12 @@ struct rf_handle {
 
 namespace rf {
 rf_status fail(rf_handle *h, rf_status s, const std::string &msg);
+// preconditioner MLP inference on the tensor cores (mlp_tc.cu)
+int mlp_tc_padded_rows();
+cudaError_t mlp_tc_pad_weights(const float *w, int nout, int K, __nv_bfloat16 *out, cudaStream_t st);
+cudaError_t mlp_tc_forward(const __nv_bfloat16 *W1, const float *b1, const __nv_bfloat16 *W2, const float *b2,
+                           const __nv_bfloat16 *W3, const float *b3, int rows, int nin, int nhid, int nout,
+                           const float *X, __nv_bfloat16 *H1, __nv_bfloat16 *H2, float *O, int *err, cudaStream_t st);
 // row-block shards (shard.cu)
 void shard_range(int M, int R, int r, int *t0, int *t1);
 int shard_pad(int M, int R);

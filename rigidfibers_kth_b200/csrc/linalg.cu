@@ -391,27 +391,45 @@ __global__ void gather_rows_kernel(const T *A, int64_t lda, int64_t row0, int64_
     }
 }
 
-// z_i = v_i + sum_{m < kp} B_{i,m} v_{j_m}: one thread per output entry (i, r);
-// B row-major blocks, pstride blocks per fiber; j_m = knn[i * kstride + m]
-// (negative: no neighbour).  FP64 accumulation in a fixed order.
+// z_i = v_i + sum_{m < kp} B_{i,m} v_{j_m}.  A CTA owns kApplyFibers fibers:
+// it first stages their neighbour lists and the neighbours' entries of v in
+// shared memory (independent, coalesced loads), then one thread per output
+// entry (i, r) runs over the blocks' rows; B row-major blocks, pstride blocks
+// per fiber; j_m = knn[i * kstride + m] (negative: no neighbour).  FP64
+// accumulation in a fixed order.  Needs nb <= 24 and kp <= 8.
+constexpr int kApplyFibers = 16;
+constexpr int kApplyMaxNb = 24;
+constexpr int kApplyMaxKp = 8;
 template <typename T>
-__global__ void pair_apply_kernel(int M, int nb, int kp, int pstride, const float *__restrict__ B,
-                                  const int *__restrict__ knn, int kstride, const T *__restrict__ v, T *__restrict__ z,
-                                  const int *__restrict__ stop) {
+__global__ void __launch_bounds__(kApplyFibers * kApplyMaxNb) pair_apply_kernel(
+    int M, int nb, int kp, int pstride, const float *__restrict__ B, const int *__restrict__ knn, int kstride,
+    const T *__restrict__ v, T *__restrict__ z, const int *__restrict__ stop) {
     if (stop && *stop) return;
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)M * nb) return;
-    const int64_t i = idx / nb;
-    const int r = (int)(idx - i * nb);
-    double s = (double)v[idx];
+    __shared__ int s_j[kApplyFibers * kApplyMaxKp];
+    __shared__ T s_v[kApplyFibers * kApplyMaxKp * kApplyMaxNb];
+    const int f0 = blockIdx.x * kApplyFibers;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int t = tid; t < kApplyFibers * kp; t += nt) {
+        const int f = t / kp, m = t - f * kp;
+        s_j[t] = (f0 + f < M) ? knn[(int64_t)(f0 + f) * kstride + m] : -1;
+    }
+    __syncthreads();
+    for (int t = tid; t < kApplyFibers * kp * nb; t += nt) {
+        const int q = t / nb, c = t - q * nb;
+        const int j = s_j[q];
+        s_v[t] = j >= 0 ? v[(int64_t)j * nb + c] : (T)0;
+    }
+    __syncthreads();
+    const int f = tid / nb, r = tid - f * nb;
+    const int64_t i = f0 + f;
+    if (f >= kApplyFibers || i >= M) return;
+    double s = (double)v[i * nb + r];
     for (int m = 0; m < kp; ++m) {
-        const int j = knn[i * kstride + m];
-        if (j < 0) continue;
         const float *b = B + ((i * pstride + m) * nb + r) * nb;
-        const T *vj = v + (int64_t)j * nb;
+        const T *vj = s_v + (f * kp + m) * nb;
         for (int c = 0; c < nb; ++c) s += (double)b[c] * (double)vj[c];
     }
-    z[idx] = (T)s;
+    z[i * nb + r] = (T)s;
 }
 
 inline unsigned grid_for(int64_t n) {
@@ -503,9 +521,9 @@ cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t ro
 template <typename T>
 cudaError_t launch_pair_apply(int M, int nb, int kp, int pstride, const float *B, const int *knn, int kstride,
                               const T *v, T *z, cudaStream_t st, const int *stop) {
-    const int64_t tot = (int64_t)M * nb;
-    pair_apply_kernel<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(M, nb, kp, pstride, B, knn, kstride, v, z,
-                                                                         stop);
+    if (nb > kApplyMaxNb || kp > kApplyMaxKp) return cudaErrorInvalidValue;
+    pair_apply_kernel<T><<<(unsigned)((M + kApplyFibers - 1) / kApplyFibers), kApplyFibers * nb, 0, st>>>(
+        M, nb, kp, pstride, B, knn, kstride, v, z, stop);
     return cudaGetLastError();
 }
 

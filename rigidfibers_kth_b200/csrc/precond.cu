@@ -605,7 +605,16 @@ rf_status apply_mlp(rf_handle *h) {
     if ((s = ensure_mlp_buffers(h)) != RF_OK) return s;
     if ((s = ck(launch_pair_features(h), "features")) != RF_OK) return s;
     const int rows = M * kPair;
-    if ((s = ck(mlp_forward(h->mlp_w, rows, h->feat, h->mlp_h1, h->mlp_h2, h->mlp_out, st), "mlp")) != RF_OK) return s;
+    // inference on the tensor cores (BF16 operands, FP32 accumulation); the
+    // FP32 CUDA-core GEMMs remain for training
+    const MlpLayout Lw;
+    const int P = mlp_tc_padded_rows();
+    __nv_bfloat16 *w1 = h->mlp_wtc, *w2 = w1 + (size_t)P * kIn, *w3 = w2 + (size_t)P * kHid;
+    if ((s = ck(mlp_tc_forward(w1, h->mlp_w + Lw.b1, w2, h->mlp_w + Lw.b2, w3, h->mlp_w + Lw.b3, rows, kIn, kHid, kOut,
+                               h->feat, reinterpret_cast<__nv_bfloat16 *>(h->mlp_h1),
+                               reinterpret_cast<__nv_bfloat16 *>(h->mlp_h2), h->mlp_out, h->mlp_err, st),
+                "mlp")) != RF_OK)
+        return s;
     pair_frame_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(M, kPair, feat_rot(h), feat_sign(h), h->mlp_out,
                                                                        kOut, h->Pblocks, kOut, 1);
     h->launches += 4;
@@ -646,6 +655,19 @@ rf_status rf_set_mlp_weights(rf_handle *h, const float *weights, int64_t count) 
         return fail(h, RF_ERR_OOM, "alloc weights");
     if (cudaMemcpy(h->mlp_w, weights, sizeof(float) * count, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(h, RF_ERR_CUDA, "upload weights");
+    // BF16 copies of W1, W2, W3 with their rows padded to the tensor-core tile
+    const MlpLayout Lw;
+    const int P = mlp_tc_padded_rows();
+    if (!h->mlp_wtc && (cudaMalloc(&h->mlp_wtc, sizeof(__nv_bfloat16) * (size_t)P * (kIn + 2 * kHid)) != cudaSuccess ||
+                        cudaMalloc(&h->mlp_err, sizeof(int)) != cudaSuccess))
+        return fail(h, RF_ERR_OOM, "alloc weights");
+    __nv_bfloat16 *w1 = h->mlp_wtc, *w2 = w1 + (size_t)P * kIn, *w3 = w2 + (size_t)P * kHid;
+    if (mlp_tc_pad_weights(h->mlp_w + Lw.w1, kHid, kIn, w1, h->stream) != cudaSuccess ||
+        mlp_tc_pad_weights(h->mlp_w + Lw.w2, kHid, kHid, w2, h->stream) != cudaSuccess ||
+        mlp_tc_pad_weights(h->mlp_w + Lw.w3, kOut, kHid, w3, h->stream) != cudaSuccess ||
+        cudaMemsetAsync(h->mlp_err, 0, sizeof(int), h->stream) != cudaSuccess ||
+        cudaStreamSynchronize(h->stream) != cudaSuccess)
+        return fail(h, RF_ERR_CUDA, "convert weights");
     h->mlp_loaded = true;
     h->pc_ready = false;
     return RF_OK;
@@ -694,6 +716,49 @@ rf_status rf_compute_cluster_targets(rf_handle *h, float *targets) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "targets");
     if (saved != RF_PC_CLUSTER) h->pc_ready = false;
+    return RF_OK;
+}
+
+rf_status rf_mlp_predict(int32_t device, const float *weights, const float *features, int64_t count, float *out) {
+    if (!weights || !features || !out || count < 1 || count > (1 << 22))
+        return fail(nullptr, RF_ERR_INVALID_ARG, "rf_mlp_predict: bad arguments");
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(nullptr, RF_ERR_NO_DEVICE, "no CUDA device");
+    }
+    const MlpLayout Lw;
+    const int P = mlp_tc_padded_rows();
+    float *w = nullptr, *x = nullptr, *o = nullptr;
+    __nv_bfloat16 *wt = nullptr, *h1 = nullptr, *h2 = nullptr;
+    int *err = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&w, sizeof(float) * Lw.total);
+    if (e == cudaSuccess) e = cudaMalloc(&x, sizeof(float) * count * kIn);
+    if (e == cudaSuccess) e = cudaMalloc(&o, sizeof(float) * count * kOut);
+    if (e == cudaSuccess) e = cudaMalloc(&wt, sizeof(__nv_bfloat16) * (size_t)P * (kIn + 2 * kHid));
+    if (e == cudaSuccess) e = cudaMalloc(&h1, sizeof(__nv_bfloat16) * count * kHid);
+    if (e == cudaSuccess) e = cudaMalloc(&h2, sizeof(__nv_bfloat16) * count * kHid);
+    if (e == cudaSuccess) e = cudaMalloc(&err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w, weights, sizeof(float) * Lw.total, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(x, features, sizeof(float) * count * kIn, cudaMemcpyHostToDevice, st);
+    __nv_bfloat16 *w1 = wt, *w2 = w1 + (size_t)P * kIn, *w3 = w2 + (size_t)P * kHid;
+    if (e == cudaSuccess) e = mlp_tc_pad_weights(w + Lw.w1, kHid, kIn, w1, st);
+    if (e == cudaSuccess) e = mlp_tc_pad_weights(w + Lw.w2, kHid, kHid, w2, st);
+    if (e == cudaSuccess) e = mlp_tc_pad_weights(w + Lw.w3, kOut, kHid, w3, st);
+    if (e == cudaSuccess)
+        e = mlp_tc_forward(w1, w + Lw.b1, w2, w + Lw.b2, w3, w + Lw.b3, (int)count, kIn, kHid, kOut, x, h1, h2, o, err,
+                           st);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, o, sizeof(float) * count * kOut, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    void *ptrs[] = {w, x, o, wt, h1, h2, err};
+    for (void *p : ptrs) cudaFree(p);
+    if (st) cudaStreamDestroy(st);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "rf_mlp_predict");
+    if (herr) return fail(nullptr, RF_ERR_DEVICE_TIMEOUT, "rf_mlp_predict: tensor-core wait timed out");
     return RF_OK;
 }
 

@@ -15,12 +15,13 @@
 // The all-gather wants equal counts: each shard's block is padded to the
 // largest block, and a compaction kernel puts the blocks in row order.
 //
-// NCCL is loaded at run time (dlopen of libnccl.so.2; an already loaded copy
-// is reused), so the library itself has no link dependency on it.
+// NCCL is loaded at run time (dlopen: RF_NCCL_LIBRARY, or an already loaded
+// copy, or libnccl.so.2), so the library itself has no link dependency on it.
 #include <dlfcn.h>
 #include <nccl.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -42,9 +43,14 @@ namespace {
 NcclApi g_nccl;
 std::string g_nccl_err;
 
+// The NCCL library: RF_NCCL_LIBRARY (a path) if set, else the copy already in
+// the process (e.g. the one PyTorch loads: a second, older copy under the same
+// name would break a later import of PyTorch), else libnccl.so.2.
 bool load_nccl() {
     if (g_nccl.lib) return true;
-    void *lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+    void *lib = nullptr;
+    if (const char *path = getenv("RF_NCCL_LIBRARY")) lib = dlopen(path, RTLD_NOW | RTLD_GLOBAL);
+    if (!lib) lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
     if (!lib) lib = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
     if (!lib) lib = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
     if (!lib) {

@@ -76,6 +76,16 @@ class Trainer:
             pass
 
 
+def predict(weights, features, device=0):
+    """The network's output (count x 225) as the preconditioner computes it:
+    BF16 tensor-core inference (rf_mlp_predict)."""
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    x = np.ascontiguousarray(features, dtype=np.float32)
+    out = np.zeros((x.shape[0], 225), dtype=np.float32)
+    L.check(L.lib().rf_mlp_predict(device, _f(w), _f(x), x.shape[0], _f(out)))
+    return out
+
+
 def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=8, device=0):
     """Pair features and exact cluster-inverse coupling blocks of one seeded
     Gaussian cloud ((M * 8) rows each)."""

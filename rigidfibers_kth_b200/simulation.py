@@ -154,9 +154,20 @@ def shard_range(M, shard_count, shard_index):
     return t0.value, t1.value
 
 
+def _load_torch_nccl():
+    """Make the library use PyTorch's NCCL: the library loads NCCL at run time
+    and reuses a copy already in the process; loading an older system copy
+    first would break a later ``import torch`` in the same process."""
+    try:
+        import torch  # noqa: F401  (loads its NCCL with libtorch_cuda)
+    except ImportError:
+        pass
+
+
 def shard_unique_id():
     """A new NCCL id (128 bytes) for the shards' communicator; made on one rank
     and sent to the others by the caller (e.g. torch.distributed)."""
+    _load_torch_nccl()
     buf = ctypes.create_string_buffer(128)
     L.check(L.lib().rf_shard_unique_id(buf))
     return buf.raw
@@ -188,6 +199,7 @@ class Simulation:
             st = L.lib().rf_create(ctypes.byref(self._c), _ptr(pos), _ptr(ori), ctypes.byref(h))
         else:
             assert len(nccl_id) == 128
+            _load_torch_nccl()
             st = L.lib().rf_create_sharded(ctypes.byref(self._c), _ptr(pos), _ptr(ori), bytes(nccl_id), ctypes.byref(h))
         L.check(st, None)
         self._h = h

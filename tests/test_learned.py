@@ -211,3 +211,40 @@ def test_shipped_weights_load_and_solve():
     # against the FP64 method the FP32 far field moves the answer by ~1e-7 of its scale;
     # the velocity bound of the mixed path is 1e-6
     assert np.abs(x1 - x0).max() <= 1e-6 * np.abs(x0).max()
+
+
+def _bf16(a):
+    """Round to BF16 (nearest, ties to even), returned as float64."""
+    u = np.ascontiguousarray(a, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
+    return u.view(np.float32).astype(np.float64)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("count", [1, 1000])
+def test_tensor_core_inference_matches_bf16_reference(count):
+    """The preconditioner's inference (tcgen05 MMAs, BF16 operands, FP32
+    accumulation in tensor memory, 128-row tiles; 1000 rows leave a partial
+    tile) against numpy with the same roundings: inputs, weights and hidden
+    activations rounded to BF16, sums in FP64.  The FP32 sums of the tensor
+    cores and the FP64 sums of numpy round a few hidden activations to
+    neighbouring BF16 values (2^-8 apart), which moves the outputs by up to
+    ~2e-4 of their largest value: bound 1e-3, far below the BF16 effect
+    itself (the inference is within 5e-2 of the FP32 network)."""
+    import os
+
+    from rigidfibers_kth_b200.learned import predict
+
+    w = np.load(os.path.join(os.path.dirname(rf.__file__), "mlp_weights.npy")).astype(np.float64)
+    pos, ori = rf.generate_layout(200, "gaussian", 1.7, 0.2, seed=1620)
+    with rf.Simulation(rf.Configuration(rf.FiberParams(slenderness=1e-3), pos, ori)) as sim:
+        X = sim.features()[:count]
+    got = predict(w.astype(np.float32), X).astype(np.float64)
+    W1, b1, W2, b2, W3, b3 = mlp_ref.unpack(w)
+    h1 = _bf16(np.maximum(_bf16(X) @ _bf16(W1).T + b1, 0.0))
+    h2 = _bf16(np.maximum(h1 @ _bf16(W2).T + b2, 0.0))
+    want = h2 @ _bf16(W3).T + b3
+    scale = np.abs(want).max()
+    assert np.abs(got - want).max() <= 1e-3 * scale, np.abs(got - want).max() / scale
+    _, _, fp32 = mlp_ref.forward(w, X)
+    assert np.abs(got - fp32).max() <= 5e-2 * np.abs(fp32).max()
