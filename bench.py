@@ -23,6 +23,13 @@ Arms:
                      GMRES solve, velocities and advection), so their summed
                      time is a measured step; nothing is extrapolated.  It
                      never loads the product library.
+  --impl reference-gpu
+                     the reference's own CUDA program (oracle/_ref/fibers_gpu,
+                     built unmodified from its sources) on the only case it is
+                     compiled for, the M=100 golden case, beside this
+                     library's plain FP64 path on the same case.  Not the
+                     benchmark workload: the program's sizes are compile-time
+                     constants.
 
 Multi-GPU: every rank runs an independent replica (the reference has no
 parallelism beyond one device); value = steps of all ranks / max time.
@@ -88,7 +95,7 @@ def parse_args():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--impl", choices=["ours", "reference", "reference-gpu"], default="ours")
     ap.add_argument("--M", type=int, default=WORKLOAD["M"], help="override the number of fibers (smoke runs)")
     ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
     ap.add_argument("--pc", choices=["learned", "cluster", "none"], default="learned")
@@ -239,6 +246,32 @@ def timed_steps(sim, steps, warmup, world, first_index=0, collect_stats=False):
     launches = sim.kernel_launches() - launches0
     barrier(world)
     return ms, (stats if collect_stats else launches), t
+
+
+def read_only_bandwidth(device, gib=4, reps=5):
+    """HBM bandwidth of a read-only stream on this GPU: a reduction over a
+    buffer far larger than L2 (torch's sum kernel), best of `reps`, CUDA
+    events.  The product kernels only read A, so this is the ceiling they
+    are compared with beside the measured copy bandwidth."""
+    try:
+        import torch
+
+        x = torch.ones(gib * (1 << 28), dtype=torch.float32, device=f"cuda:{device}")
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        best = None
+        for _ in range(reps + 1):
+            s.record()
+            x.sum()
+            e.record()
+            e.synchronize()
+            ms = s.elapsed_time(e)
+            best = ms if best is None else min(best, ms)
+        del x
+        torch.cuda.empty_cache()
+        return gib * (1 << 30) / (best * 1e-3) / 1e9
+    except Exception:
+        return None
 
 
 def phase_breakdown(sim, t):
@@ -410,7 +443,9 @@ def run_ours(args):
         iters = [s["iterations"] for s in stats]
         learned = {"mean_inner_iterations": float(np.mean(iters)),
                    "mean_products": float(np.mean([s["matvecs"] for s in stats])),
-                   "solve_ms_phase_step": phases["solve"]}
+                   "solve_ms_phase_step": phases["solve"],
+                   "steps_not_converged": sum(int(not s["converged"]) for s in stats),
+                   "fallbacks_to_no_preconditioner": sum(int(s["pc_fallback"]) for s in stats)}
         # roofline of the dominant kernel: the inner-solve product (BF16 A), timed
         # live over the timed region with events on the handle's stream
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
@@ -419,11 +454,15 @@ def run_ours(args):
         per_launch = gemv_ms / max(1, gemv_count)
         achieved = gemv_bytes / (per_launch * 1e-3) / 1e9 if gemv_count else None
         n_el = float(matrix_ld) * 3 * WORKLOAD["N"] * M
+        read_peak = read_only_bandwidth(local)
         roof = {"bound": "hbm", "kernel": "gemv_partial_kernel + gemv_reduce_kernel (BF16 A x FP32 x)",
                 "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak if achieved else None,
                 "traffic": TRAFFIC_PER_ELEMENT * n_el if TRAFFIC_PER_ELEMENT else None,
-                "peak_source": "measured (copy)" if "hbm_gbs" in peaks else "fallback",
+                "peak_source": ("measured copy bandwidth (read + write bytes of a device copy; a read-only stream "
+                                "such as the product can exceed it)") if "hbm_gbs" in peaks else "fallback",
+                "read_only_peak": read_peak,
+                "frac_of_read_only": achieved / read_peak if (achieved and read_peak) else None,
                 "algorithmic_bytes": gemv_bytes, "ms_per_launch": per_launch, "launches_timed": gemv_count,
                 "share_of_timed_region": gemv_ms / ms,
                 "isolated_ms_per_launch": mv_ms}
@@ -511,7 +550,7 @@ def run_config(args):
         barrier(world)
         sim.gemv_timer(True)
         launches0 = sim.kernel_launches()
-        total_ms, iters, saved, failed = 0.0, [], [], None
+        total_ms, iters, saved, failed, unconverged, fallbacks = 0.0, [], [], None, 0, 0
         for t in range(steps):
             pre = sim.state() if (t + 1) in cfg["check"] else None
             sim.mark(0)
@@ -522,7 +561,10 @@ def run_config(args):
                 break
             sim.mark(1)
             total_ms += sim.elapsed_ms(0, 1)
-            iters.append(sim.solve_stats()["iterations"])
+            ss = sim.solve_stats()
+            iters.append(ss["iterations"])
+            unconverged += int(not ss["converged"])
+            fallbacks += int(ss["pc_fallback"])
             if pre is not None:
                 saved.append((t + 1, pre, sim.velocities()))
         count, gms, gbytes = sim.gemv_timer(False)
@@ -536,6 +578,8 @@ def run_config(args):
         arms[name] = {"value": world * done / (total_ms * 1e-3) if done else None, "unit": "steps/s",
                       "ms_per_step": total_ms / done if done else None, "steps_completed": done, "failed": failed,
                       "gmres_tol": tol, "mean_iterations": float(np.mean(iters)) if iters else None,
+                      "max_iterations": int(max(iters)) if iters else None,
+                      "steps_not_converged": unconverged, "preconditioner_fallbacks": fallbacks,
                       "gpu_launches": int(launches),
                       "products": {"bytes": gbytes, "ms_per_launch": per, "launches": count, "achieved_gbs": ach,
                                    "frac": ach / hbm_peak if ach else None,
@@ -750,10 +794,114 @@ def run_reference(args):
     }
 
 
+REF_GPU_EXE = os.path.join(ROOT, "oracle", "_ref", "fibers_gpu")
+# The one case the reference's CUDA program runs: its kernels are compiled for
+# 100 fibers, eps 0.01, N = 5 and 8 x 3 Gauss points (src/kernels/constants.cu),
+# its GMRES tolerance is fixed at 1e-5 (src/simulation.cu:337) and it stops
+# after the first time step (src/main.cu:62-65).  That is the reference's own
+# golden case: the XcT_init100.in layout with the run100_iter.in parameters
+# (v1 parameter file, one value per line, src/parameters.cc:124-180).
+REF_GPU_PARAMS = ["golden", "XcT_init100", "5", "0.01", "0.1", "10", "1", "1", "8", "1", "0", "10", "100", "1e-5"]
+REF_GPU_PHASES = ("assemble_system", "solve_system", "update_velocities", "update_fibers_firststep")
+
+
+def _ref_gpu_phases(out):
+    """Seconds per phase from the program's own event timers: lines
+    "[BENCHMARK]   : <name> : <last>(<average>) sec" (src/performance.cc)."""
+    phases = {}
+    for line in out.splitlines():
+        if "[BENCHMARK]" in line:
+            f = line.split(":")
+            if len(f) >= 3:
+                phases[f[1].strip()] = float(f[2].strip().split("(")[0])
+    return phases
+
+
+def _rel_err(a, b):
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    if a.shape != b.shape:
+        return None
+    return float(np.abs(a - b).max() / max(1e-300, np.abs(b).max()))
+
+
+def run_reference_gpu(args):
+    """The reference's own CUDA program (oracle/_ref/fibers_gpu, built from its
+    sources by oracle/Makefile) on the only case it is compiled for, beside
+    this library's plain FP64 path on the same case.  Each of the W + K runs
+    is one process that takes one (forward Euler) time step; the step time is
+    the sum of the program's own CUDA-event phase timers (assembly, ViennaCL
+    GMRES, velocities, advection; its text dump of A, b and x is not timed).
+    Accuracy: its b and x against the reference Fortran's golden vectors."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return None
+    g = np.load(os.path.join(ROOT, "tests", "golden", "golden_m100.npz"))
+    X0, T0 = g["layout_pos"], g["layout_orient"]
+    gold_b, gold_x = g["100_analytic_gmres/0_BVec"], g["100_analytic_gmres/0_XVec"]
+    config = {"workload": "reference golden case: M=100 (XcT_init100.in), eps 0.01, N=5, 8x3 Gauss points, "
+                          "GMRES(10) tol 1e-5, first (Euler) step, FP64", "M": 100, "parallelism": "single GPU"}
+    base = {"impl": "reference-gpu", "metric": "steps/s of the first time step of the M=100 golden case",
+            "unit": "steps/s", "n_gpus": 1, "higher_is_better": True, "data": "the reference's golden layout",
+            "config": config}
+    if not os.path.exists(REF_GPU_EXE):
+        return dict(base, unavailable="oracle/_ref/fibers_gpu not built (oracle/Makefile ref-gpu needs the "
+                                      "reference's sources)")
+    runs = []
+    with tempfile.TemporaryDirectory() as d:
+        par, lay = os.path.join(d, "run100_iter.in"), os.path.join(d, "XcT_init100.in")
+        with open(par, "w") as f:
+            f.write("\n".join(REF_GPU_PARAMS) + "\n")
+        with open(lay, "w") as f:
+            f.write(f"{len(X0)}\n")
+            for p, t in zip(X0, T0):
+                f.write(f"{p[0]:.16f} {p[1]:.16f} {p[2]:.16f}\n{t[0]:.16f} {t[1]:.16f} {t[2]:.16f}\n")
+        for _ in range(args.warmup + max(1, args.steps)):
+            r = subprocess.run([REF_GPU_EXE, par, lay], capture_output=True, text=True, timeout=600)
+            ph = _ref_gpu_phases(r.stdout)
+            if r.returncode != 0 or not all(n in ph for n in REF_GPU_PHASES):
+                tail = (r.stdout + r.stderr).strip().splitlines()[-3:]
+                return dict(base, unavailable=f"reference CUDA program exited {r.returncode}: {' | '.join(tail)}")
+            runs.append(ph)
+    # the program writes its last step's b and x next to itself (src/simulation.cu:468-546)
+    out_dir = os.path.dirname(REF_GPU_EXE)
+    acc = {}
+    for name, gold in (("b", gold_b), ("x", gold_x)):
+        path = os.path.join(out_dir, f"{name}_vector.out")
+        acc[name] = _rel_err(np.loadtxt(path), gold) if os.path.exists(path) else None
+    timed = runs[args.warmup:]
+    step_s = [sum(ph[n] for n in REF_GPU_PHASES) for ph in timed]
+    ref_phases = {n: 1e3 * float(np.mean([ph[n] for ph in timed])) for n in REF_GPU_PHASES}
+
+    # this library's plain FP64 path, the same case and tolerance, timed on its stream
+    import rigidfibers_kth_b200 as rf
+
+    # a fresh run each time, like the program's one step per process (GMRES
+    # from a zero initial guess; handle creation and upload not timed)
+    ours, ours_acc = [], {}
+    for k in range(args.warmup + max(1, args.steps)):
+        with rf.Simulation(rf.Configuration(rf.FiberParams(device=0), X0, T0)) as sim:
+            sim.mark(0); sim.assemble_system(); sim.mark(1); sim.solve_system(); sim.mark(2)
+            sim.update_velocities(); sim.mark(3); sim.update_fibers(True); sim.mark(4)
+            if k >= args.warmup:
+                ours.append([sim.elapsed_ms(i, i + 1) for i in range(4)])
+            ours_acc = {"b": _rel_err(sim.rhs(), gold_b), "x": _rel_err(sim.coeffs(), gold_x)}
+    ours = np.array(ours)
+    ours_ms = float(ours.sum(axis=1).mean())
+    ref_ms = 1e3 * float(np.mean(step_s))
+    return dict(base, value=1e3 / ref_ms, steps=len(timed), warmup=args.warmup, ms_per_step=ref_ms,
+                dtype="f64 storage (float transcendentals, src/kernels/assemble_system.cu:21)",
+                phases_ms=ref_phases, error_vs_fortran_golden=acc,
+                product_same_case={"value": 1e3 / ours_ms, "ms_per_step": ours_ms,
+                                   "phases_ms": dict(zip(REF_GPU_PHASES, map(float, ours.mean(axis=0)))),
+                                   "error_vs_fortran_golden": ours_acc,
+                                   "path": "plain FP64 (RF_PREC_FP64, CERFACS GMRES(10) tol 1e-5)"})
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         out = run_reference(args)
+    elif args.impl == "reference-gpu":
+        out = run_reference_gpu(args)
     else:
         out = run_ours(args) if args.config == 4 else run_config(args)
     if out is not None:

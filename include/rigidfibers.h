@@ -59,7 +59,11 @@ typedef enum rf_status {
 typedef enum rf_precision {
     RF_PREC_FP64 = 0,        /* plain method: FP64 assembly, FP64 A, FP64 GMRES */
     RF_PREC_FP32 = 1,        /* plain method in FP32 (reference "float" build) */
-    RF_PREC_MIXED_BF16 = 2,  /* BF16 A for inner GMRES (FP32 accumulate), FP32 A for FP64-residual refinement */
+    RF_PREC_MIXED_BF16 = 2,  /* BF16 A for inner GMRES (FP32 accumulate), FP32 A for FP64-residual refinement;
+                                a refinement that reduces the residual by less than half (BF16's
+                                2^-9 relative error times the condition of A near 1: fibers that
+                                nearly touch) switches the rest of that solve's inner products to
+                                the FP32 A (rf_solve_stats.precision_fallback) */
     RF_PREC_MIXED_FP32 = 3   /* FP32 A for inner GMRES and for the FP64-residual refinement */
 } rf_precision;
 
@@ -70,6 +74,11 @@ typedef enum rf_preconditioner {
     RF_PC_LEARNED = 2        /* the same form with B_im predicted by the MLP below; falls back to
                                 RF_PC_NONE without weights */
 } rf_preconditioner;
+/* Every preconditioned (inner) GMRES solve first gets a trial budget of
+ * max(3 * restart, 30) Arnoldi steps; a solve that has not converged by then
+ * goes on from its iterate without the preconditioner (RF_PC_NONE, block
+ * Jacobi), so a poor block never changes the tolerance a solve reaches
+ * (rf_solve_stats.pc_fallback records it). */
 
 typedef enum rf_velocity_mode {
     RF_VEL_RECOMPUTE = 0,    /* re-evaluate the pair integrals with the solved forces (reference) */
@@ -124,6 +133,9 @@ typedef struct rf_solve_stats {
     int32_t refinements;      /* outer FP64-residual refinements (mixed precision) */
     double residual;          /* final true ||b-Ax||/||b|| */
     double seconds;           /* device time of the solve */
+    int32_t pc_fallback;      /* 1 if the preconditioned solve missed its trial budget and the
+                                 solve went on without the preconditioner (see RF_PC_CLUSTER) */
+    int32_t precision_fallback; /* 1 if RF_PREC_MIXED_BF16 switched its inner products to the FP32 A */
 } rf_solve_stats;
 
 typedef struct rf_handle rf_handle;

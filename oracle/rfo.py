@@ -35,9 +35,17 @@ class RfoParams(ctypes.Structure):
     ]
 
 
-def build():
-    """Compile the oracle with its Makefile (g++, OpenMP)."""
+def build(reference="/root/reference"):
+    """Compile the oracle with its Makefile (g++, OpenMP); where the
+    reference's sources are present, also its own CUDA program (_ref/, the
+    reference-gpu arm of bench.py).  A failure of that second build is
+    reported and leaves the oracle usable."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    if os.path.isdir(os.path.join(reference, "src")):
+        r = subprocess.run(["make", "-s", "-C", _HERE, "ref-gpu", f"REFERENCE={reference}"],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            print("reference CUDA program not built:", (r.stdout + r.stderr)[-400:])
 
 
 def lib():

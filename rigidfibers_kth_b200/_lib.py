@@ -73,6 +73,8 @@ class RfSolveStats(ctypes.Structure):
         ("refinements", ctypes.c_int32),
         ("residual", ctypes.c_double),
         ("seconds", ctypes.c_double),
+        ("pc_fallback", ctypes.c_int32),
+        ("precision_fallback", ctypes.c_int32),
     ]
 
 

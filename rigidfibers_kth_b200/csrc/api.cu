@@ -650,6 +650,13 @@ rf_status rf_solve_system(rf_handle *h) {
     h->stats = rf_solve_stats();
     CK(h, cudaEventRecord(h->ev0, st), "event");
     const bool use_pc = h->p.preconditioner != RF_PC_NONE && h->pc_ready;
+    // A preconditioned solve runs in trials of pc_trial Arnoldi steps, each
+    // restarted from the current iterate; a trial that has not reduced the
+    // residual tenfold ends the preconditioner for the rest of the solve, so
+    // a poor block (a network's prediction far off its training data) costs
+    // at most a trial and never the tolerance, while a good one on a hard
+    // system (slow but steady) is kept.
+    const int pc_trial = std::max(3 * m, 30);
     const int nb = 3 * h->N;
     rf::GmresResult res;
     rf_status status = RF_OK;
@@ -715,7 +722,27 @@ rf_status rf_solve_system(rf_handle *h) {
             return rf::launch_pair_apply<double>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
                                                   h->stream);
         };
-        CK(h, h->gm64->solve(A, use_pc ? &P : nullptr, h->b, h->x, false, tol, maxit, &res), "GMRES");
+        {
+            bool pc_on = use_pc;
+            double prev = 1.0;  // residual relative to |b| before this trial
+            rf::GmresResult part;
+            for (int used = 0;;) {
+                const int budget = pc_on ? std::min(maxit - used, pc_trial) : maxit - used;
+                CK(h, h->gm64->solve(A, pc_on ? &P : nullptr, h->b, h->x, false, tol, budget, &part), "GMRES");
+                used += part.iterations;
+                res.iterations += part.iterations;
+                res.matvecs += part.matvecs;
+                res.launches += part.launches;
+                res.info = part.info;
+                res.backward_error = part.backward_error;
+                if (part.info != rf::kInfoBudget || used >= maxit || part.iterations == 0) break;
+                if (pc_on && part.backward_error > 0.1 * prev) {
+                    pc_on = false;
+                    h->stats.pc_fallback = 1;
+                }
+                prev = part.backward_error;
+            }
+        }
         if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
         h->launches += res.launches;
         h->stats.iterations = res.iterations;
@@ -737,7 +764,27 @@ rf_status rf_solve_system(rf_handle *h) {
         CK(h, (rf::launch_convert<float, double>(h->n, h->x, h->x32, st)), "convert");
         CK(h, (rf::launch_convert<float, double>(h->n, h->b, h->r32, st)), "convert");
         h->launches += 2;
-        CK(h, h->gm32->solve(A, use_pc ? &P : nullptr, h->r32, h->x32, false, tol, maxit, &res), "GMRES");
+        {
+            bool pc_on = use_pc;
+            double prev = 1.0;  // residual relative to |b| before this trial
+            rf::GmresResult part;
+            for (int used = 0;;) {
+                const int budget = pc_on ? std::min(maxit - used, pc_trial) : maxit - used;
+                CK(h, h->gm32->solve(A, pc_on ? &P : nullptr, h->r32, h->x32, false, tol, budget, &part), "GMRES");
+                used += part.iterations;
+                res.iterations += part.iterations;
+                res.matvecs += part.matvecs;
+                res.launches += part.launches;
+                res.info = part.info;
+                res.backward_error = part.backward_error;
+                if (part.info != rf::kInfoBudget || used >= maxit || part.iterations == 0) break;
+                if (pc_on && part.backward_error > 0.1 * prev) {
+                    pc_on = false;
+                    h->stats.pc_fallback = 1;
+                }
+                prev = part.backward_error;
+            }
+        }
         if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
         CK(h, (rf::launch_convert<double, float>(h->n, h->x32, h->x, st)), "convert");
         h->launches += res.launches + 1;
@@ -750,8 +797,9 @@ rf_status rf_solve_system(rf_handle *h) {
         // vectors and accumulation, FP64 Hessenberg/Givens), outer iterative
         // refinement with the residual b - A x accumulated in FP64 against
         // the FP32-stored matrix.
-        const bool bf16 = prec == RF_PREC_MIXED_BF16;
-        rf::Gmres<float>::Op Alo = [h, bf16](const float *in, float *out) {
+        // BF16 while the refinements make progress, then the FP32 A
+        bool bf16 = prec == RF_PREC_MIXED_BF16;
+        rf::Gmres<float>::Op Alo = [h, &bf16](const float *in, float *out) {
             h->launches += 2;
             return timed_product(h, (bf16 ? 2.0 : 4.0) * h->lda * h->n, [&] {
                 if (bf16)
@@ -768,7 +816,7 @@ rf_status rf_solve_system(rf_handle *h) {
         };
         // the same operators for the device-controlled inner solve: their
         // kernels return at once once the solve has stopped
-        rf::Gmres<float>::StopOp Alo_s = [h, bf16](const float *in, float *out, const int *stop) {
+        rf::Gmres<float>::StopOp Alo_s = [h, &bf16](const float *in, float *out, const int *stop) {
             h->launches += 2;
             return timed_product(h, (bf16 ? 2.0 : 4.0) * h->lda * h->n, [&] {
                 if (bf16)
@@ -829,6 +877,7 @@ rf_status rf_solve_system(rf_handle *h) {
         if (e == cudaSuccess && !(std::isfinite(bn) && std::isfinite(rn)))
             return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
         int it = 0, iters = 0;
+        bool pc_on = use_pc;
         const int max_ref = h->p.max_refinements > 0 ? h->p.max_refinements : 30;
         const double itol = h->p.inner_tol > 0.0 ? std::min(h->p.inner_tol, 0.5) : 1e-3;
         while (e == cudaSuccess && bn > 0.0 && rn / bn > tol && it < max_ref && iters < maxit * max_ref) {
@@ -847,22 +896,42 @@ rf_status rf_solve_system(rf_handle *h) {
             const double need = 0.5 * tol * bn / rn;
             const int left = std::max(1, (int)std::ceil(std::log(need) / std::log(itol) - 1e-9));
             const double itol_k = std::min(0.5, std::pow(need, 1.0 / left));
+            const int budget = pc_on ? std::min(maxit, pc_trial) : maxit;
             if (device_control)
-                e = h->gm32->solve_device(Alo_s, use_pc ? &P_s : nullptr, h->r32, h->d32, itol_k, maxit, &res,
+                e = h->gm32->solve_device(Alo_s, pc_on ? &P_s : nullptr, h->r32, h->d32, itol_k, budget, &res,
                                           drop_skipped);
             else
-                e = h->gm32->solve(Alo, use_pc ? &P : nullptr, h->r32, h->d32, true, itol_k, maxit, &res, false);
+                e = h->gm32->solve(Alo, pc_on ? &P : nullptr, h->r32, h->d32, true, itol_k, budget, &res, false);
             if (e != cudaSuccess) break;
             if (res.info == rf::kInfoNaN) return rf::fail(h, RF_ERR_NAN, "non-finite value in the linear system");
+            // a preconditioned inner solve that spent its trial keeps its partial
+            // correction (the residual is recomputed below); without a tenfold
+            // reduction (the Arnoldi estimate, relative to the unit right-hand
+            // side) the rest of this solve runs without the preconditioner
+            const bool pc_failed = pc_on && res.info == rf::kInfoBudget && budget < maxit && res.backward_error > 0.1;
+            if (pc_failed) {
+                pc_on = false;
+                h->stats.pc_fallback = 1;
+            }
             h->launches += res.launches;
             iters += res.iterations;
             h->stats.matvecs += res.matvecs;
             e = rf::launch_axpy_fd(h->n, rn, h->d32, h->x, st);
             if (e != cudaSuccess) break;
             h->launches++;
+            const double rn_prev = rn;
             e = residual();
             if (e == cudaSuccess) e = norm_of(h->r64, &rn);
             ++it;
+            // A refinement reduces the residual by about max(its inner
+            // tolerance, |I - A A_lo^-1|); less than half (when it asked for
+            // much more) means the stored BF16 matrix is too far from A for
+            // this system (its condition times BF16's 2^-9 near 1): the FP32
+            // A takes over.
+            if (e == cudaSuccess && bf16 && res.info == 0 && rn > std::max(0.5, 4.0 * itol_k) * rn_prev) {
+                bf16 = false;
+                h->stats.precision_fallback = 1;
+            }
         }
         CK(h, e, "mixed-precision solve");
         h->stats.iterations = iters;

@@ -55,16 +55,22 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = nthreads >> 5;
 
+    // w_q P_m(q) (16 x kMaxLQ, rows > N zero): the numeric inner integral reads
+    // it for every source; the analytic one only loads the tensor-core A
+    // operands from it once, so there it lives in the G region (6 KB less
+    // shared memory per CTA; the registers still hold the kernel at four CTAs
+    // per SM: capped at 128 registers for five it spills and runs 10 % slower)
+    constexpr int WP_OWN = NUMERIC || PMODE != kPModeFP64 ? 16 * kMaxLQ : 0;
     double *s_pv = reinterpret_cast<double *>(smem_raw);   // kMaxLQ
-    double *s_wP = s_pv + kMaxLQ;                           // 16 x kMaxLQ : w_q P_m(q), rows > N zero
-    double *s_xt = s_wP + 16 * kMaxLQ;                      // TI x 3
+    double *s_xt = s_pv + kMaxLQ + WP_OWN;                  // TI x 3
     double *s_tt = s_xt + TI * 3;                           // TI x 3
     double *s_acc = s_tt + TI * 3;                          // TI x NL(k) x 6: sum_j theta^k_0
     double *s_th = s_acc + TI * NL * 6;                     // TI x NL(k) x NG
     // the tensor values of P1/P2 and the staged block of P3 share one region
     double *s_G = s_th + TI * NL * NG;                      // NCOL x LDQ
     double *s_blk = s_G;                                    // CT x RT staged block
-    const int big = max(NCOL * LDQ, CT * RT + 2 * CT * TI * 3);
+    double *s_wP = WP_OWN ? s_pv + kMaxLQ : s_G;
+    const int big = max(max(NCOL * LDQ, CT * RT + 2 * CT * TI * 3), 16 * kMaxLQ);
     float *s_pvf = reinterpret_cast<float *>(s_G + big);    // kMaxLQ
     float *s_wPf = s_pvf + kMaxLQ;                          // NL x kMaxLQ
 
@@ -111,6 +117,7 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
 #pragma unroll
         for (int s = 0; s < KSMAX; ++s)
             afrag[mt][s] = s < KS ? s_wP[(mt * 8 + (lane >> 2)) * kMaxLQ + 4 * s + (lane & 3)] : 0.0;
+    if (!WP_OWN) __syncthreads();  // s_wP shares the G region the first source overwrites
 
     const int j0 = blockIdx.y * a.chunk;
     const int j1 = min(a.M, j0 + a.chunk);
@@ -423,7 +430,9 @@ static cudaError_t launch_assemble_n(const AsmArgs &a, int nchunks, cudaStream_t
     constexpr int NL = N + 1, NG = NL * 6;
     const int LQ = a.LQ, LDQ = round_up_int(LQ, 4) + 2;
     const size_t big = std::max((size_t)TI * NG * LDQ, (size_t)(3 * N) * (TI * 3 * N) + 2 * (3 * N) * (TI * 3));
-    size_t smem = sizeof(double) * (kMaxLQ + 16 * kMaxLQ + TI * 3 * 2 + TI * NL * 6 + TI * NL * NG + big);
+    constexpr int WP_OWN = NUMERIC || PMODE != kPModeFP64 ? 16 * kMaxLQ : 0;
+    size_t smem = sizeof(double) * (kMaxLQ + WP_OWN + TI * 3 * 2 + TI * NL * 6 + TI * NL * NG +
+                                    std::max(big, (size_t)(16 * kMaxLQ)));
     smem += sizeof(float) * (kMaxLQ + NL * kMaxLQ);
     const int threads = round_up_int(TI * LQ, 32);
     auto kern = threads <= 96 ? assemble_kernel<N, NUMERIC, PMODE, 96, kMinBlocks96>

@@ -549,31 +549,58 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
         for (int pp = 0; pp < NV; ++pp)
 #pragma unroll
             for (int k = 0; k < KW; ++k) V[pp][k] = 0.f;
+        // the Gauss point q's moments, weighted, into the projections
+        auto add_point = [&](int q, const float *I, const float *J, const float *S) {
+            const float *w = s_w + q * KW;
+            float wk[KW];
+#pragma unroll
+            for (int k = 0; k < KW; ++k) wk[k] = w[k];
+#pragma unroll
+            for (int pp = 0; pp < NL; ++pp) {
+                const float u = fmaf(e2, J[pp], I[pp]);
+#pragma unroll
+                for (int k = 0; k < NL; ++k) U[pp][k] = fmaf(wk[k], u, U[pp][k]);
+            }
+#pragma unroll
+            for (int pp = 0; pp < NV; ++pp) {
+                const float v = fmaf(-e6, S[pp], J[pp]);
+#pragma unroll
+                for (int k = 0; k < KW; ++k)
+                    if (k < vrows(N, pp)) V[pp][k] = fmaf(wk[k], v, V[pp][k]);
+            }
+        };
         if (act) {
-            // two Gauss points in flight (two independent recursions): 2 % faster
-            // once the warps of a scheduler share the instruction stream
-#pragma unroll 2
-            for (int q = 0; q < LQ; ++q) {
-                const float sq = s_pv[q];
-                const float r0x = fmaf(sq, t[0], D[0]), r0y = fmaf(sq, t[1], D[1]), r0z = fmaf(sq, t[2], D[2]);
-                float I[KW], J[KW], S[KW];
-                moments_fp32<N, FAR>(Geom32(r0x, r0y, r0z, p[0], p[1], p[2]), I, J, S);
-                const float *w = s_w + q * KW;
-                float wk[KW];
+            if constexpr (FAR) {
+                // every point far (c >= 6): two Gauss points per pass of the
+                // packed recursion, added in the order q, q + 1.  Past an odd LQ
+                // the partner is the zero padding of s_pv: computed, not added.
+                static_assert(kMaxLQ % 2 == 0, "the partner of the last point must lie in s_pv");
+                for (int q = 0; q < LQ; q += 2) {
+                    const float sa = s_pv[q], sb = s_pv[q + 1];
+                    const Geom32 ga(fmaf(sa, t[0], D[0]), fmaf(sa, t[1], D[1]), fmaf(sa, t[2], D[2]), p[0], p[1], p[2]);
+                    const Geom32 gb(fmaf(sb, t[0], D[0]), fmaf(sb, t[1], D[1]), fmaf(sb, t[2], D[2]), p[0], p[1], p[2]);
+                    float2 I2[KW], J2[KW], S2[KW];
+                    moments_backward_fp32x2<N>(make_float2(ga.b, gb.b), make_float2(ga.c, gb.c), I2, J2, S2);
+                    float I[KW], J[KW], S[KW];
 #pragma unroll
-                for (int k = 0; k < KW; ++k) wk[k] = w[k];
+                    for (int k = 0; k < KW; ++k) { I[k] = I2[k].x; J[k] = J2[k].x; S[k] = S2[k].x; }
+                    add_point(q, I, J, S);
+                    if (q + 1 < LQ) {
 #pragma unroll
-                for (int pp = 0; pp < NL; ++pp) {
-                    const float u = fmaf(e2, J[pp], I[pp]);
-#pragma unroll
-                    for (int k = 0; k < NL; ++k) U[pp][k] = fmaf(wk[k], u, U[pp][k]);
+                        for (int k = 0; k < KW; ++k) { I[k] = I2[k].y; J[k] = J2[k].y; S[k] = S2[k].y; }
+                        add_point(q + 1, I, J, S);
+                    }
                 }
-#pragma unroll
-                for (int pp = 0; pp < NV; ++pp) {
-                    const float v = fmaf(-e6, S[pp], J[pp]);
-#pragma unroll
-                    for (int k = 0; k < KW; ++k)
-                        if (k < vrows(N, pp)) V[pp][k] = fmaf(wk[k], v, V[pp][k]);
+            } else {
+                // two Gauss points in flight (two independent recursions): 2 % faster
+                // once the warps of a scheduler share the instruction stream
+#pragma unroll 2
+                for (int q = 0; q < LQ; ++q) {
+                    const float sq = s_pv[q];
+                    const float r0x = fmaf(sq, t[0], D[0]), r0y = fmaf(sq, t[1], D[1]), r0z = fmaf(sq, t[2], D[2]);
+                    float I[KW], J[KW], S[KW];
+                    moments_fp32<N, FAR>(Geom32(r0x, r0y, r0z, p[0], p[1], p[2]), I, J, S);
+                    add_point(q, I, J, S);
                 }
             }
         }

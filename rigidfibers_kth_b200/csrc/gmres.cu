@@ -166,7 +166,7 @@ cudaError_t Gmres<VT>::solve_device(const StopOp &A, const StopOp *P, const VT *
         RF_TRY(launch_add<VT>(n_, x, upd, x, st_));
         res->launches++;
         if (last_stop) {
-            res->info = last_stop == 1 ? 0 : -4;
+            res->info = last_stop == 1 ? 0 : kInfoBudget;
             return cudaSuccess;
         }
         // restart from the residual of the updated x
@@ -324,7 +324,7 @@ cudaError_t Gmres<VT>::solve(const Op &A, const Op *P, const VT *b, VT *x, bool 
                     RF_TRY(cudaMemcpyAsync(x, xcur_, sizeof(VT) * n_, cudaMemcpyDeviceToDevice, st_));
                     RF_TRY(cudaStreamSynchronize(st_));
                     res->backward_error = bea;
-                    res->info = bea <= tol ? 0 : -4;
+                    res->info = bea <= tol ? 0 : kInfoBudget;
                     return cudaSuccess;
                 }
                 RF_TRY(residual(A, b, xcur_, w_, res));
@@ -337,7 +337,7 @@ cudaError_t Gmres<VT>::solve(const Op &A, const Op *P, const VT *b, VT *x, bool 
                     RF_TRY(cudaMemcpyAsync(x, xcur_, sizeof(VT) * n_, cudaMemcpyDeviceToDevice, st_));
                     RF_TRY(cudaStreamSynchronize(st_));
                     res->backward_error = be;
-                    res->info = be <= tol ? 0 : -4;
+                    res->info = be <= tol ? 0 : kInfoBudget;
                     return cudaSuccess;
                 }
             }

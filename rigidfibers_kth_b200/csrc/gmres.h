@@ -19,6 +19,7 @@
 
 namespace rf {
 
+constexpr int kInfoBudget = -4;
 constexpr int kInfoNaN = -5;
 
 struct GmresResult {

@@ -183,6 +183,47 @@ __device__ __forceinline__ void moments_backward_fp32(float b, float c, float *I
     }
 }
 
+// The same recursion for two points at once on Blackwell's packed FP32 units
+// (__ffma2_rn / __fmul2_rn: one instruction, two FMAs, each rounded exactly as
+// fmaf): component .x is one point, .y the other, every operation and its
+// order as in moments_backward_fp32, so the moments are bit-identical.
+template <int N>
+__device__ __forceinline__ void moments_backward_fp32x2(float2 b, float2 c, float2 *I, float2 *J, float2 *S) {
+    constexpr int K = N + 3;
+    const float xe0 = 1.0f + b.x + c.x, xb0 = 1.0f - b.x + c.x;
+    const float xe1 = 1.0f + b.y + c.y, xb1 = 1.0f - b.y + c.y;
+    const float ue0 = xe0 * rsqrtf(xe0), ub0 = xb0 * rsqrtf(xb0);
+    const float ue1 = xe1 * rsqrtf(xe1), ub1 = xb1 * rsqrtf(xb1);
+    const float ic0 = __fdividef(1.0f, c.x), ic1 = __fdividef(1.0f, c.y);
+    const float2 ic = make_float2(ic0, ic1);
+    const float2 icb = make_float2(ic0 * b.x, ic1 * b.y);
+    const float2 icwp = make_float2(__fdividef(2.0f * b.x, ue0 + ub0) * ic0, __fdividef(2.0f * b.y, ue1 + ub1) * ic1);
+    const float2 icwm = make_float2((ue0 + ub0) * ic0, (ue1 + ub1) * ic1);
+    const float2 nic = make_float2(-ic0, -ic1), nicb = make_float2(-icb.x, -icb.y);
+    const float2 ic2 = make_float2(ic0 * ic0, ic1 * ic1);
+    const float2 z = make_float2(0.f, 0.f);
+    float2 i1 = z, i2 = z, j1 = z, j2 = z, s1 = z, s2 = z;
+#pragma unroll
+    for (int n = kBackTop; n >= 0; --n) {
+        const float a0 = (n + 2.0f) / (n + 1.0f);
+        const float r2 = 1.0f / (n + 2.0f);
+        const float cb = (1.0f - 2.0f * (n + 2.0f)) / (2.0f * (n + 2.0f));
+        const float2 icw = ((n + 1) % 2 == 0) ? icwp : icwm;
+        const float2 ca = __fmul2_rn(make_float2(a0 * cb, a0 * cb), icb);
+        const float2 cn = __fmul2_rn(make_float2(-a0, -a0), ic);
+        const float2 cw = __fmul2_rn(make_float2(a0 * r2, a0 * r2), icw);
+        const float2 in = __ffma2_rn(ca, i1, __ffma2_rn(cn, i2, cw));
+        const float2 jn = __ffma2_rn(nicb, j1, __ffma2_rn(nic, j2, in));
+        const float2 sn = __ffma2_rn(nicb, s1, __ffma2_rn(nic, s2, jn));
+        if (n < K) {
+            I[n] = in;
+            J[n] = __fmul2_rn(jn, ic);
+            S[n] = __fmul2_rn(sn, ic2);
+        }
+        i2 = i1; i1 = in; j2 = j1; j1 = jn; s2 = s1; s1 = sn;
+    }
+}
+
 // Geometry of one (target point, source fiber) item in FP32 for the moments:
 // b = -2 p.R0, c = |R0|^2, and the three quantities that the closed forms
 // need near the source and that c and b determine only through cancellation:

@@ -292,7 +292,8 @@ class Simulation:
         s = L.RfSolveStats()
         L.check(L.lib().rf_get_solve_stats(self._h, ctypes.byref(s)), self._h)
         return dict(converged=bool(s.converged), iterations=s.iterations, matvecs=s.matvecs,
-                    refinements=s.refinements, residual=s.residual, seconds=s.seconds)
+                    refinements=s.refinements, residual=s.residual, seconds=s.seconds,
+                    pc_fallback=bool(s.pc_fallback), precision_fallback=bool(s.precision_fallback))
 
     def history(self):
         a = [np.zeros(3 * self.M) for _ in range(4)]

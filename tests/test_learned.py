@@ -248,3 +248,24 @@ def test_tensor_core_inference_matches_bf16_reference(count):
     assert np.abs(got - want).max() <= 1e-3 * scale, np.abs(got - want).max() / scale
     _, _, fp32 = mlp_ref.forward(w, X)
     assert np.abs(got - fp32).max() <= 5e-2 * np.abs(fp32).max()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [rf.PREC_FP64, rf.PREC_MIXED_BF16])
+def test_poor_blocks_fall_back_to_no_preconditioner(prec):
+    """Weights far off the trained ones (the shipped weights x 50: coupling
+    blocks thousands of times too large) make the preconditioned operator so
+    ill-conditioned that GMRES stalls; the solve misses its trial budget,
+    goes on without the preconditioner from its iterate and still reaches
+    the tolerance with the answer of the unpreconditioned method."""
+    import os
+
+    w = np.load(os.path.join(os.path.dirname(rf.__file__), "mlp_weights.npy")) * 50.0
+    pos, ori = rf.generate_layout(300, "gaussian", 3.0 * (300 / 4000) ** (1 / 3), 0.2, seed=1603)
+    x0, s0 = _solve(pos, ori, rf.PC_NONE, prec=prec)
+    x1, s1 = _solve(pos, ori, rf.PC_LEARNED, weights=w, prec=prec)
+    assert s1["converged"] and s1["pc_fallback"], s1
+    assert not s0["pc_fallback"]
+    assert s1["residual"] <= 1e-10
+    # both are solutions of the same system to a relative residual of 1e-10
+    assert np.abs(x1 - x0).max() <= 1e-8 * np.abs(x0).max()
