@@ -100,6 +100,8 @@ def parse_args():
     ap.add_argument("--precision", choices=["bf16", "fp32"], default="bf16")
     ap.add_argument("--pc", choices=["learned", "cluster", "none"], default="learned")
     ap.add_argument("--weights", default=os.path.join(ROOT, "rigidfibers_kth_b200", "mlp_weights.npy"))
+    ap.add_argument("--pc-damping", type=float, default=None,
+                    help="damping of the preconditioner's coupling blocks (default: the library's)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=4,
@@ -217,11 +219,17 @@ def workload_config(M, world):
 
 
 # ---------------------------------------------------------------- product arm
+# block damping (FiberParams.pc_damping) of the preconditioned arms; None: the library's default
+PC_DAMPING = None
+
+
 def make_sim(rf, pos, ori, device, precision, pc, velocity_mode, tol=WORKLOAD["tol"]):
     p = rf.FiberParams(slenderness=WORKLOAD["eps"], timestep=WORKLOAD["dt"],
                        num_terms_in_force_expansion=WORKLOAD["N"], num_quadrature_intervals=WORKLOAD["NoQI"],
                        gmres_restart=WORKLOAD["restart"], gmres_tol=tol, gmres_max_iters=300,
                        precision=precision, preconditioner=pc, velocity_mode=velocity_mode, device=device)
+    if PC_DAMPING is not None:
+        p.pc_damping = PC_DAMPING
     return rf.Simulation(rf.Configuration(p, pos, ori))
 
 
@@ -445,7 +453,8 @@ def run_ours(args):
                    "mean_products": float(np.mean([s["matvecs"] for s in stats])),
                    "solve_ms_phase_step": phases["solve"],
                    "steps_not_converged": sum(int(not s["converged"]) for s in stats),
-                   "fallbacks_to_no_preconditioner": sum(int(s["pc_fallback"]) for s in stats)}
+                   "fallbacks_to_no_preconditioner": sum(int(s["pc_fallback"]) for s in stats),
+                   "steps_preconditioned": sum(int(s["preconditioned"]) for s in stats)}
         # roofline of the dominant kernel: the inner-solve product (BF16 A), timed
         # live over the timed region with events on the handle's stream
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
@@ -484,6 +493,7 @@ def run_ours(args):
             "config": workload_config(M, world),
             "arm": {"precision": args.precision + " A (inner GMRES) + FP32 A (FP64-accumulated residual) + FP64 "
                                  "refinement", "preconditioner": args.pc,
+                    "pc_damping": PC_DAMPING if PC_DAMPING is not None else "library default",
                     "velocities": "stored P0/P1 projection panels"},
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -521,6 +531,8 @@ def config_sim(rf, cfg, pos, ori, device, precision, tol, pc, velocity_mode):
                        num_quadrature_intervals=8, gmres_restart=10, gmres_tol=tol,
                        gmres_max_iters=300 if tol >= 1e-10 else 2000, precision=precision, preconditioner=pc,
                        velocity_mode=velocity_mode, device=device)
+    if PC_DAMPING is not None:
+        p.pc_damping = PC_DAMPING
     return rf.Simulation(rf.Configuration(p, pos, ori))
 
 
@@ -550,7 +562,7 @@ def run_config(args):
         barrier(world)
         sim.gemv_timer(True)
         launches0 = sim.kernel_launches()
-        total_ms, iters, saved, failed, unconverged, fallbacks = 0.0, [], [], None, 0, 0
+        total_ms, iters, saved, failed, unconverged, fallbacks, preconditioned = 0.0, [], [], None, 0, 0, 0
         for t in range(steps):
             pre = sim.state() if (t + 1) in cfg["check"] else None
             sim.mark(0)
@@ -565,6 +577,7 @@ def run_config(args):
             iters.append(ss["iterations"])
             unconverged += int(not ss["converged"])
             fallbacks += int(ss["pc_fallback"])
+            preconditioned += int(ss["preconditioned"])
             if pre is not None:
                 saved.append((t + 1, pre, sim.velocities()))
         count, gms, gbytes = sim.gemv_timer(False)
@@ -580,6 +593,7 @@ def run_config(args):
                       "gmres_tol": tol, "mean_iterations": float(np.mean(iters)) if iters else None,
                       "max_iterations": int(max(iters)) if iters else None,
                       "steps_not_converged": unconverged, "preconditioner_fallbacks": fallbacks,
+                      "steps_preconditioned": preconditioned,
                       "gpu_launches": int(launches),
                       "products": {"bytes": gbytes, "ms_per_launch": per, "launches": count, "achieved_gbs": ach,
                                    "frac": ach / hbm_peak if ach else None,
@@ -897,7 +911,9 @@ def run_reference_gpu(args):
 
 
 def main():
+    global PC_DAMPING
     args = parse_args()
+    PC_DAMPING = args.pc_damping
     if args.impl == "reference":
         out = run_reference(args)
     elif args.impl == "reference-gpu":

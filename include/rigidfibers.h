@@ -74,11 +74,17 @@ typedef enum rf_preconditioner {
     RF_PC_LEARNED = 2        /* the same form with B_im predicted by the MLP below; falls back to
                                 RF_PC_NONE without weights */
 } rf_preconditioner;
-/* Every preconditioned (inner) GMRES solve first gets a trial budget of
- * max(3 * restart, 30) Arnoldi steps; a solve that has not converged by then
- * goes on from its iterate without the preconditioner (RF_PC_NONE, block
- * Jacobi), so a poor block never changes the tolerance a solve reaches
- * (rf_solve_stats.pc_fallback records it). */
+/* A preconditioned (inner) GMRES solve runs in trials of max(3 * restart, 30)
+ * Arnoldi steps, each restarted from the current iterate; a trial without a
+ * tenfold reduction of the residual ends the preconditioner for the rest of
+ * that solve, which goes on without it (RF_PC_NONE, block Jacobi), so a poor
+ * block never changes the tolerance a solve reaches
+ * (rf_solve_stats.pc_fallback records it).  The blocks are kept only while
+ * they pay: the handle keeps running means of its solves' iterations with
+ * and without them; after a solve that fell back, or while the mean with
+ * them is above the one without, the next 8 assemblies neither build nor use
+ * them, and while they pay one solve in 32 runs without them to keep the
+ * comparison current (rf_solve_stats.preconditioned). */
 
 typedef enum rf_velocity_mode {
     RF_VEL_RECOMPUTE = 0,    /* re-evaluate the pair integrals with the solved forces (reference) */
@@ -122,7 +128,11 @@ typedef struct rf_params {
                                             (rf_shard_range) and keeps all state replicated; FP64,
                                             GMRES, recomputed velocities, no block preconditioner.  Solve and
                                             velocities need the shards' communicator (rf_create_sharded). */
-    int32_t reserved[6];
+    double pc_damping;                   /* block preconditioners: z_i = v_i + pc_damping sum_m B_im v_(j_m)
+                                            (default 0.75; 0 selects the default).  The coupling blocks of
+                                            a local cluster inverse overshoot where the couplings are
+                                            strong (settled, dense states); damped they help there too */
+    int32_t reserved[4];
 } rf_params;
 
 /* GMRES / refinement statistics of the last solve. */
@@ -136,6 +146,8 @@ typedef struct rf_solve_stats {
     int32_t pc_fallback;      /* 1 if the preconditioned solve missed its trial budget and the
                                  solve went on without the preconditioner (see RF_PC_CLUSTER) */
     int32_t precision_fallback; /* 1 if RF_PREC_MIXED_BF16 switched its inner products to the FP32 A */
+    int32_t preconditioned;   /* 1 if the solve started with the block preconditioner */
+    int32_t reserved;
 } rf_solve_stats;
 
 typedef struct rf_handle rf_handle;

@@ -61,7 +61,8 @@ class RfParams(ctypes.Structure):
         ("near_field_c", ctypes.c_double),
         ("shard_index", ctypes.c_int32),
         ("shard_count", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("pc_damping", ctypes.c_double),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -75,6 +76,8 @@ class RfSolveStats(ctypes.Structure):
         ("seconds", ctypes.c_double),
         ("pc_fallback", ctypes.c_int32),
         ("precision_fallback", ctypes.c_int32),
+        ("preconditioned", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

@@ -155,6 +155,21 @@ namespace {
 // Mixed solves that start from zero after a warm start left more than 10 %
 // of |b|; the next one tries the warm start again.
 constexpr int kWarmRetry = 8;
+// The block preconditioner is kept only while it pays.  The solver keeps a
+// running mean of the iterations of its solves with and without it; after a
+// solve whose blocks missed a trial (see rf_solve_system), or whose mean is
+// above the mean without them, the next kPcRetry assemblies neither build
+// nor use them.  While the blocks pay, one solve in kPcExplore runs without
+// them to keep that comparison current (the suspension's state drifts).
+constexpr int kPcRetry = 8;
+// Default damping of the neighbour blocks, z_i = v_i + 0.75 sum_m B_im v_(j_m):
+// measured on the M = 4000 cloud over 30 steps the learned blocks give the
+// same iterations for damping 0.75 .. 1 (20, 20, 18, 18 at steps 0, 10, 20,
+// 30; 23-25 without), the exact cluster blocks 20 / 18 at 0.7 against 32 / 29
+// undamped; on the uniform M = 8000 box (dt 0.05) 33 and 42 at steps 10 and
+// 30 against 36 and 70 undamped and 42 and 54 without.
+constexpr double kPcDamping = 0.75;
+constexpr int kPcExplore = 32;
 
 
 // Sum the recorded start/stop pairs of the product timer (waits for them).
@@ -225,6 +240,7 @@ void rf_params_default(rf_params *p) {
     p->cluster_size = 8;
     p->inner_tol = 1e-3;
     p->near_field_c = 6.0;
+    p->pc_damping = kPcDamping;
 }
 
 const char *rf_status_string(rf_status s) {
@@ -260,6 +276,8 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown preconditioner");
     if (p->velocity_mode != RF_VEL_RECOMPUTE && p->velocity_mode != RF_VEL_REUSE)
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "unknown velocity mode");
+    if (!(p->pc_damping >= 0.0 && p->pc_damping <= 2.0))
+        return rf::fail(nullptr, RF_ERR_INVALID_ARG, "pc_damping must be in [0, 2] (0: the default)");
     if (M < 2 && p->preconditioner != RF_PC_NONE)
         return rf::fail(nullptr, RF_ERR_INVALID_ARG, "a block preconditioner needs at least two fibers");
     if (p->use_direct_solver && p->precision != RF_PREC_FP64)
@@ -293,6 +311,7 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
 
     rf_handle *h = new rf_handle;
     h->p = *p;
+    if (h->p.pc_damping == 0.0) h->p.pc_damping = kPcDamping;
     h->M = M;
     h->N = N;
     h->LQ = 3 * NoQI;
@@ -606,7 +625,10 @@ rf_status rf_assemble_system(rf_handle *h) {
         h->vpart_chunks = h->asm_chunks;
         h->launches += 2;
     }
-    if (h->p.preconditioner != RF_PC_NONE) {
+    if (h->p.preconditioner != RF_PC_NONE && (h->pc_skips > 0 || h->pc_age >= kPcExplore)) {
+        if (h->pc_skips > 0) --h->pc_skips;
+        h->pc_ready = false;
+    } else if (h->p.preconditioner != RF_PC_NONE) {
         rf_status s = rf::build_preconditioner(h);
         if (s != RF_OK) return s;
     }
@@ -657,6 +679,8 @@ rf_status rf_solve_system(rf_handle *h) {
     // at most a trial and never the tolerance, while a good one on a hard
     // system (slow but steady) is kept.
     const int pc_trial = std::max(3 * m, 30);
+    h->stats.preconditioned = use_pc ? 1 : 0;
+    const double pc_omega = h->p.pc_damping;
     const int nb = 3 * h->N;
     rf::GmresResult res;
     rf_status status = RF_OK;
@@ -718,8 +742,8 @@ rf_status rf_solve_system(rf_handle *h) {
                                                                        h->stream);
             });
         };
-        rf::Gmres<double>::Op P = [h, nb](const double *in, double *out) {
-            return rf::launch_pair_apply<double>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+        rf::Gmres<double>::Op P = [h, nb, pc_omega](const double *in, double *out) {
+            return rf::launch_pair_apply<double>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, pc_omega, in, out,
                                                   h->stream);
         };
         {
@@ -757,8 +781,8 @@ rf_status rf_solve_system(rf_handle *h) {
                                                                    h->work32, h->work_elems, h->sm_count, h->stream);
             });
         };
-        rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
-            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+        rf::Gmres<float>::Op P = [h, nb, pc_omega](const float *in, float *out) {
+            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, pc_omega, in, out,
                                                  h->stream);
         };
         CK(h, (rf::launch_convert<float, double>(h->n, h->x, h->x32, st)), "convert");
@@ -810,8 +834,8 @@ rf_status rf_solve_system(rf_handle *h) {
                                                                    h->work32, h->work_elems, h->sm_count, h->stream);
             });
         };
-        rf::Gmres<float>::Op P = [h, nb](const float *in, float *out) {
-            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+        rf::Gmres<float>::Op P = [h, nb, pc_omega](const float *in, float *out) {
+            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, pc_omega, in, out,
                                                  h->stream);
         };
         // the same operators for the device-controlled inner solve: their
@@ -828,8 +852,8 @@ rf_status rf_solve_system(rf_handle *h) {
                                                                    stop);
             });
         };
-        rf::Gmres<float>::StopOp P_s = [h, nb](const float *in, float *out, const int *stop) {
-            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, in, out,
+        rf::Gmres<float>::StopOp P_s = [h, nb, pc_omega](const float *in, float *out, const int *stop) {
+            return rf::launch_pair_apply<float>(h->M, nb, h->pc_pairs, RF_MLP_PAIRS, h->Pblocks, h->knn, RF_MLP_K, pc_omega, in, out,
                                                  h->stream, stop);
         };
         // a product queued after the inner solve stopped returns at once: not a product to time
@@ -944,6 +968,17 @@ rf_status rf_solve_system(rf_handle *h) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.seconds = ms * 1e-3;
+    if (h->p.preconditioner != RF_PC_NONE && h->stats.converged) {
+        double &mean = h->pc_its[use_pc ? 1 : 0];
+        mean = mean < 0.0 ? h->stats.iterations : 0.5 * (mean + h->stats.iterations);
+        if (!use_pc) {
+            h->pc_age = 0;
+        } else {
+            ++h->pc_age;
+            if (h->stats.pc_fallback || (h->pc_its[0] >= 0.0 && h->pc_its[1] > 1.05 * h->pc_its[0]))
+                h->pc_skips = kPcRetry;
+        }
+    }
     if (!h->stats.converged) status = rf::fail(h, RF_ERR_NOT_CONVERGED, "GMRES budget spent above tolerance");
     return status;
 }

@@ -114,6 +114,9 @@ struct rf_handle {
 
     rf_solve_stats stats{};
     int cold_solves = 0;  // mixed solves left that start from zero (poor warm start seen)
+    int pc_skips = 0;     // solves left that skip the block preconditioner
+    double pc_its[2] = {-1.0, -1.0};  // running mean of solve iterations without / with it (-1: none yet)
+    int pc_age = 0;       // preconditioned solves since the last one without it
     bool assembled = false;
     int64_t launches = 0;
     std::string err;

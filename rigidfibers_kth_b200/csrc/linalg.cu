@@ -391,7 +391,7 @@ __global__ void gather_rows_kernel(const T *A, int64_t lda, int64_t row0, int64_
     }
 }
 
-// z_i = v_i + sum_{m < kp} B_{i,m} v_{j_m}.  A CTA owns kApplyFibers fibers:
+// z_i = v_i + omega sum_{m < kp} B_{i,m} v_{j_m}.  A CTA owns kApplyFibers fibers:
 // it first stages their neighbour lists and the neighbours' entries of v in
 // shared memory (independent, coalesced loads), then one thread per output
 // entry (i, r) runs over the blocks' rows; B row-major blocks, pstride blocks
@@ -403,7 +403,7 @@ constexpr int kApplyMaxKp = 8;
 template <typename T>
 __global__ void __launch_bounds__(kApplyFibers * kApplyMaxNb) pair_apply_kernel(
     int M, int nb, int kp, int pstride, const float *__restrict__ B, const int *__restrict__ knn, int kstride,
-    const T *__restrict__ v, T *__restrict__ z, const int *__restrict__ stop) {
+    double omega, const T *__restrict__ v, T *__restrict__ z, const int *__restrict__ stop) {
     if (stop && *stop) return;
     __shared__ int s_j[kApplyFibers * kApplyMaxKp];
     __shared__ T s_v[kApplyFibers * kApplyMaxKp * kApplyMaxNb];
@@ -423,13 +423,13 @@ __global__ void __launch_bounds__(kApplyFibers * kApplyMaxNb) pair_apply_kernel(
     const int f = tid / nb, r = tid - f * nb;
     const int64_t i = f0 + f;
     if (f >= kApplyFibers || i >= M) return;
-    double s = (double)v[i * nb + r];
+    double s = 0.0;
     for (int m = 0; m < kp; ++m) {
         const float *b = B + ((i * pstride + m) * nb + r) * nb;
         const T *vj = s_v + (f * kp + m) * nb;
         for (int c = 0; c < nb; ++c) s += (double)b[c] * (double)vj[c];
     }
-    z[i * nb + r] = (T)s;
+    z[i * nb + r] = (T)fma(omega, s, (double)v[i * nb + r]);
 }
 
 inline unsigned grid_for(int64_t n) {
@@ -520,10 +520,10 @@ cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t ro
 }
 template <typename T>
 cudaError_t launch_pair_apply(int M, int nb, int kp, int pstride, const float *B, const int *knn, int kstride,
-                              const T *v, T *z, cudaStream_t st, const int *stop) {
+                              double omega, const T *v, T *z, cudaStream_t st, const int *stop) {
     if (nb > kApplyMaxNb || kp > kApplyMaxKp) return cudaErrorInvalidValue;
     pair_apply_kernel<T><<<(unsigned)((M + kApplyFibers - 1) / kApplyFibers), kApplyFibers * nb, 0, st>>>(
-        M, nb, kp, pstride, B, knn, kstride, v, z, stop);
+        M, nb, kp, pstride, B, knn, kstride, omega, v, z, stop);
     return cudaGetLastError();
 }
 
@@ -559,9 +559,9 @@ template cudaError_t launch_gather_rows<float>(const float *, int64_t, int64_t, 
                                                cudaStream_t);
 template cudaError_t launch_gather_rows<__nv_bfloat16>(const __nv_bfloat16 *, int64_t, int64_t, int64_t, int64_t,
                                                        double *, cudaStream_t);
-template cudaError_t launch_pair_apply<double>(int, int, int, int, const float *, const int *, int, const double *,
-                                               double *, cudaStream_t, const int *);
-template cudaError_t launch_pair_apply<float>(int, int, int, int, const float *, const int *, int, const float *,
-                                              float *, cudaStream_t, const int *);
+template cudaError_t launch_pair_apply<double>(int, int, int, int, const float *, const int *, int, double,
+                                               const double *, double *, cudaStream_t, const int *);
+template cudaError_t launch_pair_apply<float>(int, int, int, int, const float *, const int *, int, double,
+                                              const float *, float *, cudaStream_t, const int *);
 
 }  // namespace rf

@@ -184,11 +184,11 @@ cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t ro
                                cudaStream_t st);
 
 // ---- neighbour-block preconditioner (FP32 blocks) -----------------------------
-// z_i = v_i + sum_{m < kp} B[i][m] v_{knn[i][m]}, B[i][m] row-major 3N x 3N,
-// pstride blocks per fiber, kstride neighbours per fiber in knn
+// z_i = v_i + omega sum_{m < kp} B[i][m] v_{knn[i][m]}, B[i][m] row-major
+// 3N x 3N, pstride blocks per fiber, kstride neighbours per fiber in knn
 template <typename T>
 cudaError_t launch_pair_apply(int M, int nb, int kp, int pstride, const float *B, const int *knn, int kstride,
-                              const T *v, T *z, cudaStream_t st, const int *stop = nullptr);
+                              double omega, const T *v, T *z, cudaStream_t st, const int *stop = nullptr);
 
 // ---- device-controlled Arnoldi steps (arnoldi.cu) -------------------------------
 // State of one GMRES(m) solve held on the device: the Hessenberg columns after

@@ -86,10 +86,9 @@ def predict(weights, features, device=0):
     return out
 
 
-def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=8, device=0):
-    """Pair features and exact cluster-inverse coupling blocks of one seeded
-    Gaussian cloud ((M * 8) rows each)."""
-    pos, ori = generate_layout(M, "gaussian", sigma, 0.2, seed=seed)
+def layout_samples(pos, ori, eps=1e-3, cluster_size=8, device=0):
+    """Pair features and exact cluster-inverse coupling blocks of one layout
+    ((M * 8) rows each), from its FP64 system."""
     p = FiberParams(slenderness=eps, device=device, cluster_size=cluster_size)
     with Simulation(Configuration(p, pos, ori)) as sim:
         sim.assemble_system()
@@ -98,17 +97,52 @@ def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=8, device=0):
     return x, y
 
 
-def generate_dataset(n_samples, seed0=5000, m_range=(250, 2000), density_sigma4000=3.0, rng_seed=0, **kw):
-    """n_samples pairs from seeded clouds of M in m_range with the density of
-    the M=4000, sigma=3 cloud (sigma scaled by (M/4000)^(1/3), jittered by
-    +-20 %); seeds start at seed0 (disjoint from the evaluation seeds
-    1000-1999)."""
+def cloud_samples(M, sigma, seed, eps=1e-3, cluster_size=8, device=0):
+    """Pair features and exact cluster-inverse coupling blocks of one seeded
+    Gaussian cloud ((M * 8) rows each)."""
+    pos, ori = generate_layout(M, "gaussian", sigma, 0.2, seed=seed)
+    return layout_samples(pos, ori, eps, cluster_size, device)
+
+
+def evolve(pos, ori, steps, dt=0.1, eps=1e-3, device=0):
+    """The layout after `steps` time steps of the suspension (mixed-precision
+    path, no preconditioner): the sedimented states a run goes through."""
+    if steps <= 0:
+        return pos, ori
+    p = FiberParams(slenderness=eps, timestep=dt, gmres_tol=1e-10, gmres_max_iters=300, device=device,
+                    precision=L.PREC_MIXED_BF16, velocity_mode=L.VEL_REUSE)
+    with Simulation(Configuration(p, pos, ori)) as sim:
+        for t in range(steps):
+            sim.step(t)
+        P, O = sim.state()
+    return P.reshape(-1, 3), O.reshape(-1, 3)
+
+
+def generate_dataset(n_samples, seed0=5000, m_range=(250, 2000), density_sigma4000=3.0, rng_seed=0,
+                     kinds=("cloud",), max_steps=0, **kw):
+    """n_samples pairs from seeded layouts of M in m_range; seeds start at
+    seed0 (disjoint from the evaluation seeds 1000-1999).  Each layout is one
+    of `kinds`: "cloud", a Gaussian cloud of the density of the M=4000,
+    sigma=3 cloud (sigma scaled by (M/4000)^(1/3), jittered by +-20 %), or
+    "box", centres uniform in a cube of 8 fibers per unit volume (the
+    uniform configurations' density, jittered by +-30 %); with max_steps > 0
+    the layout is first evolved by 0..max_steps time steps (dt 0.1 or 0.05)."""
     rng = np.random.default_rng(rng_seed)
     xs, ys, total, k = [], [], 0, 0
     while total < n_samples:
         M = int(rng.integers(m_range[0], m_range[1] + 1))
-        sigma = density_sigma4000 * (M / 4000.0) ** (1 / 3) * float(rng.uniform(0.8, 1.2))
-        x, y = cloud_samples(M, sigma, seed0 + k, **kw)
+        kind = kinds[int(rng.integers(len(kinds)))]
+        if kind == "cloud":
+            sigma = density_sigma4000 * (M / 4000.0) ** (1 / 3) * float(rng.uniform(0.8, 1.2))
+            pos, ori = generate_layout(M, "gaussian", sigma, 0.2, seed=seed0 + k)
+        else:
+            box = (M / 8.0 * float(rng.uniform(0.7, 1.3))) ** (1 / 3)
+            pos, ori = generate_layout(M, "uniform", box, 0.2, seed=seed0 + k)
+        steps = int(rng.integers(0, max_steps + 1)) if max_steps > 0 else 0
+        dt = 0.1 if rng.uniform() < 0.5 else 0.05
+        dev = kw.get("device", 0)
+        pos, ori = evolve(pos, ori, steps, dt, kw.get("eps", 1e-3), dev)
+        x, y = layout_samples(pos, ori, **kw)
         xs.append(x)
         ys.append(y)
         total += len(x)
@@ -116,8 +150,9 @@ def generate_dataset(n_samples, seed0=5000, m_range=(250, 2000), density_sigma40
     return np.concatenate(xs)[:n_samples], np.concatenate(ys)[:n_samples]
 
 
-def train_preconditioner(n_samples=200_000, epochs=30, batch=512, lr=1e-3, seed=0, device=0, log=print):
-    X, Y = generate_dataset(n_samples, device=device)
+def train_preconditioner(n_samples=200_000, epochs=30, batch=512, lr=1e-3, seed=0, device=0, log=print,
+                         kinds=("cloud",), max_steps=0):
+    X, Y = generate_dataset(n_samples, device=device, kinds=kinds, max_steps=max_steps)
     tr = Trainer(device=device, seed=seed)
     tr.add_samples(X, Y)
     losses = []

@@ -47,6 +47,7 @@ class FiberParams:
     near_field_c: float = 6.0
     shard_index: int = 0
     shard_count: int = 1
+    pc_damping: float = 0.75
 
     def to_c(self):
         p = L.RfParams()
@@ -56,6 +57,7 @@ class FiberParams:
             "num_quadrature_intervals", "use_analytical_integration", "use_direct_solver", "gmres_restart",
             "gmres_max_iters", "gmres_tol", "precision", "preconditioner", "velocity_mode", "device",
             "max_refinements", "cluster_size", "inner_tol", "near_field_c", "shard_index", "shard_count",
+            "pc_damping",
         ):
             setattr(p, name, getattr(self, name))
         p.external_force[:] = list(self.external_force)
@@ -293,7 +295,8 @@ class Simulation:
         L.check(L.lib().rf_get_solve_stats(self._h, ctypes.byref(s)), self._h)
         return dict(converged=bool(s.converged), iterations=s.iterations, matvecs=s.matvecs,
                     refinements=s.refinements, residual=s.residual, seconds=s.seconds,
-                    pc_fallback=bool(s.pc_fallback), precision_fallback=bool(s.precision_fallback))
+                    pc_fallback=bool(s.pc_fallback), precision_fallback=bool(s.precision_fallback),
+                    preconditioned=bool(s.preconditioned))
 
     def history(self):
         a = [np.zeros(3 * self.M) for _ in range(4)]

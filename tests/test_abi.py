@@ -25,7 +25,9 @@ def test_params_default_matches_reference_run_file():
     assert p.slenderness == 0.01 and p.timestep == 0.1
     assert p.gmres_restart == 10 and p.gmres_max_iters == 100 and p.gmres_tol == 1e-5
     assert list(p.external_force) == [0.0, 0.0, -1.0]
+    assert p.pc_damping == 0.75
     assert ctypes.sizeof(L.RfParams) == 152
+    assert ctypes.sizeof(L.RfSolveStats) == 48
 
 
 def test_create_rejects_bad_arguments():
@@ -36,7 +38,8 @@ def test_create_rejects_bad_arguments():
     h = ctypes.c_void_p()
     bad = []
     for field, val in [("num_terms_in_force_expansion", 9), ("num_quadrature_intervals", 0),
-                       ("slenderness", 0.0), ("precision", 7), ("gmres_restart", 0)]:
+                       ("slenderness", 0.0), ("precision", 7), ("gmres_restart", 0), ("pc_damping", -0.5),
+                       ("pc_damping", 2.5), ("pc_damping", float("nan"))]:
         q = rf.FiberParams(num_fibers=2).to_c()
         setattr(q, field, val)
         bad.append(lib.rf_create(ctypes.byref(q), _ptr(pos), _ptr(ori), ctypes.byref(h)))
