@@ -129,7 +129,7 @@ typedef struct rf_params {
                                             GMRES, recomputed velocities, no block preconditioner.  Solve and
                                             velocities need the shards' communicator (rf_create_sharded). */
     double pc_damping;                   /* block preconditioners: z_i = v_i + pc_damping sum_m B_im v_(j_m)
-                                            (default 0.75; 0 selects the default).  The coupling blocks of
+                                            (default 0.85; 0 selects the default).  The coupling blocks of
                                             a local cluster inverse overshoot where the couplings are
                                             strong (settled, dense states); damped they help there too */
     int32_t reserved[4];

@@ -162,13 +162,16 @@ constexpr int kWarmRetry = 8;
 // nor use them.  While the blocks pay, one solve in kPcExplore runs without
 // them to keep that comparison current (the suspension's state drifts).
 constexpr int kPcRetry = 8;
-// Default damping of the neighbour blocks, z_i = v_i + 0.75 sum_m B_im v_(j_m):
-// measured on the M = 4000 cloud over 30 steps the learned blocks give the
-// same iterations for damping 0.75 .. 1 (20, 20, 18, 18 at steps 0, 10, 20,
-// 30; 23-25 without), the exact cluster blocks 20 / 18 at 0.7 against 32 / 29
-// undamped; on the uniform M = 8000 box (dt 0.05) 33 and 42 at steps 10 and
-// 30 against 36 and 70 undamped and 42 and 54 without.
-constexpr double kPcDamping = 0.75;
+// Default damping of the neighbour blocks, z_i = v_i + 0.85 sum_m B_im v_(j_m).
+// Single solves of evolved states: on the M = 4000 cloud the learned blocks
+// give the same iterations for damping 0.75 .. 1 (20, 20, 18, 17-18 at steps
+// 0, 10, 20, 30; 23-25 without); on the uniform M = 8000 box (dt 0.05) 33
+// and 45 at steps 10 and 30 against 36 and 70 undamped and 42 and 54
+// without; the exact cluster blocks 20 / 18 at 0.7 against 32 / 29
+// undamped.  Whole runs: the benchmark's 20 timed steps average 19.25 /
+// 19.5 / 19.95 inner iterations at 1 / 0.85 / 0.75, the M = 8000 box's 100
+// steps 3.72 steps/s at 0.85 against 3.62 at 0.75.
+constexpr double kPcDamping = 0.85;
 constexpr int kPcExplore = 32;
 
 

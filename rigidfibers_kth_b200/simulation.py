@@ -47,7 +47,7 @@ class FiberParams:
     near_field_c: float = 6.0
     shard_index: int = 0
     shard_count: int = 1
-    pc_damping: float = 0.75
+    pc_damping: float = 0.85
 
     def to_c(self):
         p = L.RfParams()

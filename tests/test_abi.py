@@ -25,7 +25,7 @@ def test_params_default_matches_reference_run_file():
     assert p.slenderness == 0.01 and p.timestep == 0.1
     assert p.gmres_restart == 10 and p.gmres_max_iters == 100 and p.gmres_tol == 1e-5
     assert list(p.external_force) == [0.0, 0.0, -1.0]
-    assert p.pc_damping == 0.75
+    assert p.pc_damping == 0.85
     assert ctypes.sizeof(L.RfParams) == 152
     assert ctypes.sizeof(L.RfSolveStats) == 48
 
