@@ -269,3 +269,27 @@ def test_poor_blocks_fall_back_to_no_preconditioner(prec):
     assert s1["residual"] <= 1e-10
     # both are solutions of the same system to a relative residual of 1e-10
     assert np.abs(x1 - x0).max() <= 1e-8 * np.abs(x0).max()
+
+
+@pytest.mark.gpu
+def test_solver_stops_using_blocks_that_do_not_pay():
+    """After a solve whose blocks missed their trial, the next 8 assemblies
+    neither build nor use them; then they are tried again.  Every step still
+    converges to the tolerance."""
+    import os
+
+    w = np.load(os.path.join(os.path.dirname(rf.__file__), "mlp_weights.npy")) * 50.0
+    pos, ori = rf.generate_layout(300, "gaussian", 3.0 * (300 / 4000) ** (1 / 3), 0.2, seed=1604)
+    p = rf.FiberParams(slenderness=1e-3, gmres_tol=1e-10, gmres_max_iters=300, preconditioner=rf.PC_LEARNED,
+                       precision=rf.PREC_MIXED_BF16, velocity_mode=rf.VEL_REUSE)
+    used, fell = [], []
+    with rf.Simulation(rf.Configuration(p, pos, ori)) as sim:
+        sim.set_mlp_weights(w)
+        for t in range(10):
+            assert sim.step(t) == 0
+            st = sim.solve_stats()
+            assert st["converged"] and st["residual"] <= 1e-10
+            used.append(st["preconditioned"])
+            fell.append(st["pc_fallback"])
+    assert used == [True] + [False] * 8 + [True], used
+    assert fell[0] and fell[9] and not any(fell[1:9]), fell
