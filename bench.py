@@ -512,7 +512,9 @@ def run_ours(args):
                          "peak_tflops": FP32_NOMINAL_TFLOPS, "peak_source": "FP32 CUDA-core nominal",
                          "frac": ASM_FLOPS_PER_PAIR * M * (M - 1) / 1e12 / (phases["assemble"] * 1e-3)
                          / FP32_NOMINAL_TFLOPS,
-                         "written_gb": (3 * WORKLOAD["N"] * M) * 1.0 * (3 * WORKLOAD["N"] * M) * 6e-9
+                         # the matrix (BF16 with FP32 storage: two 16-bit planes, 4 bytes per
+                         # entry; FP32 storage alone: 4) and the two FP32 velocity panels
+                         "written_gb": (3 * WORKLOAD["N"] * M) * 1.0 * (3 * WORKLOAD["N"] * M) * 4e-9
                          + 2 * 3 * M * (3 * WORKLOAD["N"] * M) * 4e-9,
                          "note": "split assembly (classify, near, far, finish) of the phase step; counted work of "
                                  "the reference formulas at the initial layout"},

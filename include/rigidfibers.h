@@ -59,7 +59,9 @@ typedef enum rf_status {
 typedef enum rf_precision {
     RF_PREC_FP64 = 0,        /* plain method: FP64 assembly, FP64 A, FP64 GMRES */
     RF_PREC_FP32 = 1,        /* plain method in FP32 (reference "float" build) */
-    RF_PREC_MIXED_BF16 = 2,  /* BF16 A for inner GMRES (FP32 accumulate), FP32 A for FP64-residual refinement;
+    RF_PREC_MIXED_BF16 = 2,  /* BF16 A for inner GMRES (FP32 accumulate), FP32 A for FP64-residual refinement,
+                                held as two 16-bit planes (the BF16 matrix, rounded half away from
+                                zero, and the low halves of the FP32 words: 4 bytes per entry);
                                 a refinement that reduces the residual by less than half (BF16's
                                 2^-9 relative error times the condition of A near 1: fibers that
                                 nearly touch) switches the rest of that solve's inner products to

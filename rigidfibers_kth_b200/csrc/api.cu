@@ -22,6 +22,18 @@ cudaError_t dalloc(T **p, size_t count) {
     return cudaMalloc(reinterpret_cast<void **>(p), sizeof(T) * count);
 }
 
+// y = A x (r null) or y = r - A x over the FP32 matrix of the FP32 and mixed
+// paths: its own FP32 storage, or the two 16-bit planes of the mixed BF16 path
+template <typename X, typename ACC, typename Y>
+cudaError_t fp32_gemv(rf_handle *h, const X *x, Y *y, const Y *r, ACC *work, const int *stop = nullptr) {
+    if (h->A16lo)
+        return rf::launch_gemv<rf::SplitF32, X, ACC, Y>(reinterpret_cast<const rf::SplitF32 *>(h->A16), h->lda, h->n,
+                                                        h->n, x, y, r, work, h->work_elems, h->sm_count, h->stream,
+                                                        stop, h->a_plane);
+    return rf::launch_gemv<float, X, ACC, Y>(h->A32, h->lda, h->n, h->n, x, y, r, work, h->work_elems, h->sm_count,
+                                             h->stream, stop);
+}
+
 void free_all(rf_handle *h) {
     rf::shard_detach(h);
     for (int i = 0; i < 3; ++i) {
@@ -365,13 +377,16 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
     if (prec == RF_PREC_FP64) {
         CKC(dalloc(&h->A64, asz), "alloc A (FP64)");
         CKC(cudaMemset(h->A64, 0, asz * 8), "memset A");
+    } else if (prec == RF_PREC_MIXED_BF16) {
+        // split FP32 storage: the BF16 high plane (the inner solves' matrix)
+        // and the low plane, 4 bytes per entry in all
+        CKC(dalloc(&h->A16, 2 * asz), "alloc A (BF16 high and low planes)");
+        CKC(cudaMemset(h->A16, 0, asz * 4), "memset A");
+        h->A16lo = reinterpret_cast<unsigned short *>(h->A16) + asz;
+        h->a_plane = (int64_t)asz;
     } else {
         CKC(dalloc(&h->A32, asz), "alloc A (FP32)");
         CKC(cudaMemset(h->A32, 0, asz * 4), "memset A");
-        if (prec == RF_PREC_MIXED_BF16) {
-            CKC(dalloc(&h->A16, asz), "alloc A (BF16)");
-            CKC(cudaMemset(h->A16, 0, asz * 2), "memset A");
-        }
     }
     // assembly chunking: about 8 CTAs per SM in the grid (from the whole
     // system's targets also for a row-block shard, so that its right-hand
@@ -523,6 +538,7 @@ rf_status rf_assemble_system(rf_handle *h) {
     a.tab = h->tab;
     a.A64 = h->A64;
     a.A32 = h->A32;
+    a.A16lo = h->A16lo;
     a.A16 = h->A16;
     a.lda = h->lda;
     a.bpart = h->bpart;
@@ -553,6 +569,7 @@ rf_status rf_assemble_system(rf_handle *h) {
         sa.ori = a.ori;
         sa.tab = h->tab;
         sa.A32 = h->A32;
+        sa.A16lo = h->A16lo;
         sa.A16 = h->A16;
         sa.lda = h->lda;
         sa.PV32 = h->PV32;
@@ -780,8 +797,7 @@ rf_status rf_solve_system(rf_handle *h) {
         rf::Gmres<float>::Op A = [h](const float *in, float *out) {
             h->launches += 2;
             return timed_product(h, 4.0 * h->lda * h->n, [&] {
-                return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
-                                                                   h->work32, h->work_elems, h->sm_count, h->stream);
+                return fp32_gemv<float, float, float>(h, in, out, nullptr, h->work32);
             });
         };
         rf::Gmres<float>::Op P = [h, nb, pc_omega](const float *in, float *out) {
@@ -833,8 +849,7 @@ rf_status rf_solve_system(rf_handle *h) {
                     return rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, h->n, h->n, in, out,
                                                                                nullptr, h->work32, h->work_elems,
                                                                                h->sm_count, h->stream);
-                return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
-                                                                   h->work32, h->work_elems, h->sm_count, h->stream);
+                return fp32_gemv<float, float, float>(h, in, out, nullptr, h->work32);
             });
         };
         rf::Gmres<float>::Op P = [h, nb, pc_omega](const float *in, float *out) {
@@ -850,9 +865,7 @@ rf_status rf_solve_system(rf_handle *h) {
                     return rf::launch_gemv<__nv_bfloat16, float, float, float>(h->A16, h->lda, h->n, h->n, in, out,
                                                                                nullptr, h->work32, h->work_elems,
                                                                                h->sm_count, h->stream, stop);
-                return rf::launch_gemv<float, float, float, float>(h->A32, h->lda, h->n, h->n, in, out, nullptr,
-                                                                   h->work32, h->work_elems, h->sm_count, h->stream,
-                                                                   stop);
+                return fp32_gemv<float, float, float>(h, in, out, nullptr, h->work32, stop);
             });
         };
         rf::Gmres<float>::StopOp P_s = [h, nb, pc_omega](const float *in, float *out, const int *stop) {
@@ -879,8 +892,7 @@ rf_status rf_solve_system(rf_handle *h) {
         auto residual = [&]() -> cudaError_t {  // r64 = b - A32 x (FP64 accumulation)
             h->launches += 2;
             h->stats.matvecs++;
-            return rf::launch_gemv<float, double, double, double>(h->A32, h->lda, h->n, h->n, h->x, h->r64, h->b,
-                                                                  h->work64, h->work_elems, h->sm_count, st);
+            return fp32_gemv<double, double, double>(h, h->x, h->r64, h->b, h->work64);
         };
         double bn = 0.0, rn = 0.0;
         cudaError_t e = norm_of(h->b, &bn);
@@ -1124,7 +1136,10 @@ rf_status rf_get_matrix(rf_handle *h, double *A) {
         if (h->A64) {
             e = cudaMemcpyAsync(A + c * n, h->A64 + c * h->lda, n * 8, cudaMemcpyDeviceToHost, h->stream);
         } else {
-            e = rf::launch_convert<double, float>(n, h->A32 + c * h->lda, col, h->stream);
+            e = h->A16lo ? rf::launch_gather_rows<rf::SplitF32>(reinterpret_cast<const rf::SplitF32 *>(h->A16) +
+                                                                    c * h->lda, h->lda, 0, n, 1, col, h->stream,
+                                                                h->a_plane)
+                         : rf::launch_convert<double, float>(n, h->A32 + c * h->lda, col, h->stream);
             if (e == cudaSuccess) e = cudaMemcpyAsync(A + c * n, col, n * 8, cudaMemcpyDeviceToHost, h->stream);
         }
     }
@@ -1149,6 +1164,9 @@ rf_status rf_get_matrix_rows(rf_handle *h, int32_t which, int64_t row0, int64_t 
     cudaError_t e;
     if (which == 1 && h->A16)
         e = rf::launch_gather_rows<__nv_bfloat16>(h->A16, h->lda, row0, rows, h->n, dev, h->stream);
+    else if (h->A16lo)
+        e = rf::launch_gather_rows<rf::SplitF32>(reinterpret_cast<const rf::SplitF32 *>(h->A16), h->lda, row0, rows,
+                                                 h->n, dev, h->stream, h->a_plane);
     else if (h->A64)
         e = rf::launch_gather_rows<double>(h->A64, h->lda, row0, rows, h->n, dev, h->stream);
     else

@@ -354,7 +354,10 @@ __global__ void __launch_bounds__(MAXT, MINB) assemble_kernel(AsmArgs a) {
                 if (rl >= rows_valid) continue;
                 const double v0 = s_blk[e], v1 = s_blk[e + 1];
                 const int64_t idx = (col0 + cl) * a.lda + row0 + rl;
-                if (rl + 1 < rows_valid) {
+                if (a.A16lo) {  // split FP32 storage: the two 16-bit planes
+                    split_store((float)v0, a.A16 + idx, a.A16lo + idx);
+                    if (rl + 1 < rows_valid) split_store((float)v1, a.A16 + idx + 1, a.A16lo + idx + 1);
+                } else if (rl + 1 < rows_valid) {
                     if (a.A64) *reinterpret_cast<double2 *>(a.A64 + idx) = make_double2(v0, v1);
                     if (a.A32) *reinterpret_cast<float2 *>(a.A32 + idx) = make_float2((float)v0, (float)v1);
                     if (a.A16)

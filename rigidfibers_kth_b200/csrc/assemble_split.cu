@@ -288,7 +288,7 @@ template <int N, bool PANELS>
 struct FarSmem {
     static constexpr int GR = 32 * 3 * N;                   // staged rows of one column
     static constexpr int PAN = 2 * 3 * 96;                  // staged panel columns
-    static constexpr int STG16 = 3 * GR / 2;                // BF16 copy of the staged columns (in floats)
+    static constexpr int STG16 = 3 * GR / 2;                // BF16 copy (split storage: low plane) of the staged columns
     static constexpr size_t kBytes = sizeof(float) * (32 * kNearWeight + 16 + 64 + kMaxLQ +
                                                       kMaxLQ * SplitDims<N>::KW + 3 * GR + (PANELS ? PAN : 0) +
                                                       STG16);
@@ -328,7 +328,27 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
         // whole column segments: the BF16 copy is staged too, then one lane
         // hands every segment to the copy engine (A32 and A16: 3 x 32 targets
         // x 3N rows; panels: 2 x 3 x 96 rows), and the warp moves on
-        if (a.A16) {
+        if (a.A16lo) {
+            // split FP32 storage: the low plane goes to the BF16 staging, the
+            // high plane over the first half of the FP32 staging it is read
+            // from (a step's writes reach only entries read by earlier steps
+            // or, behind the barrier, by this one).  (u + 0x8000) >> 16 is
+            // split_hi(u); the byte permutes pack two 16-bit halves.
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(stg);
+            uint2 *dh = reinterpret_cast<uint2 *>(const_cast<float *>(stg));
+            uint2 *dl = reinterpret_cast<uint2 *>(stg16);
+            for (int e0 = 0; e0 < 3 * GR / 4; e0 += 32) {
+                const int e = e0 + lane;
+                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                if (e < 3 * GR / 4) v = s4[e];
+                __syncwarp();
+                if (e < 3 * GR / 4) {
+                    dh[e] = make_uint2(__byte_perm(v.x + 0x8000u, v.y + 0x8000u, 0x7632),
+                                       __byte_perm(v.z + 0x8000u, v.w + 0x8000u, 0x7632));
+                    dl[e] = make_uint2(__byte_perm(v.x, v.y, 0x5410), __byte_perm(v.z, v.w, 0x5410));
+                }
+            }
+        } else if (a.A16) {
             const float4 *s4 = reinterpret_cast<const float4 *>(stg);
             uint2 *d2 = reinterpret_cast<uint2 *>(stg16);
             for (int e = lane; e < 3 * GR / 4; e += 32) {
@@ -347,7 +367,14 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
             for (int bb = 0; bb < 3; ++bb) {
                 const int64_t col = col0 + bb;
                 if (a.A32) bulk_s2g(a.A32 + col * a.lda + row0, stg + bb * GR, GR * sizeof(float));
-                if (a.A16) bulk_s2g(a.A16 + col * a.lda + row0, stg16 + bb * GR, GR * sizeof(__nv_bfloat16));
+                if (a.A16lo) {
+                    bulk_s2g(a.A16 + col * a.lda + row0, reinterpret_cast<const unsigned short *>(stg) + bb * GR,
+                             GR * sizeof(unsigned short));
+                    bulk_s2g(a.A16lo + col * a.lda + row0, reinterpret_cast<const unsigned short *>(stg16) + bb * GR,
+                             GR * sizeof(unsigned short));
+                } else if (a.A16) {
+                    bulk_s2g(a.A16 + col * a.lda + row0, stg16 + bb * GR, GR * sizeof(__nv_bfloat16));
+                }
                 if (PANELS) {
 #pragma unroll
                     for (int w = 0; w < 2; ++w)
@@ -364,8 +391,13 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
         const int64_t col = col0 + bb;
         const float *src = stg + bb * GR;
         for (int e = lane; e < nrows; e += 32) {
-            if (a.A32) a.A32[col * a.lda + row0 + e] = src[e];
-            if (a.A16) a.A16[col * a.lda + row0 + e] = __float2bfloat16_rn(src[e]);
+            const int64_t idx = col * a.lda + row0 + e;
+            if (a.A16lo) {
+                split_store(src[e], a.A16 + idx, a.A16lo + idx);
+            } else {
+                if (a.A32) a.A32[idx] = src[e];
+                if (a.A16) a.A16[idx] = __float2bfloat16_rn(src[e]);
+            }
         }
         if (PANELS) {
             const int prow = 3 * nvalid;
@@ -946,8 +978,12 @@ __global__ void __launch_bounds__(kNearWarps * 32, RF_NEAR_MINB) near_pairs_kern
                 if (r < 3 * RB) {
                     const int col = 3 * mm + r / RB, rr = r % RB;
                     const int64_t idx = ((int64_t)j * RB + col) * a.lda + (int64_t)i * RB + rr;
-                    if (a.A32) a.A32[idx] = v;
-                    if (a.A16) a.A16[idx] = __float2bfloat16_rn(v);
+                    if (a.A16lo) {
+                        split_store(v, a.A16 + idx, a.A16lo + idx);
+                    } else {
+                        if (a.A32) a.A32[idx] = v;
+                        if (a.A16) a.A16[idx] = __float2bfloat16_rn(v);
+                    }
                 } else if (PANELS && r < 3 * RB + 18) {
                     const int e2 = r - 3 * RB, w = e2 / 9, rem = e2 - w * 9, bb = rem / 3, aa = rem - bb * 3;
                     (w ? a.PW32 : a.PV32)[((int64_t)j * RB + 3 * mm + bb) * a.ldp + (int64_t)i * 3 + aa] = v;

@@ -42,7 +42,9 @@ struct rf_handle {
     int *lu_piv = nullptr;     // [n] pivot rows
     int *lu_info = nullptr;
     float *A32 = nullptr;
-    __nv_bfloat16 *A16 = nullptr;
+    __nv_bfloat16 *A16 = nullptr;   // BF16 matrix; in split storage also the high plane
+    unsigned short *A16lo = nullptr;  // split storage (mixed BF16): the low plane, a_plane entries after A16
+    int64_t a_plane = 0;
     double *b = nullptr;       // right-hand side
     double *x = nullptr;       // coefficients (warm start for the next solve)
     double *bpart = nullptr;   // [nchunks][n]

@@ -32,7 +32,9 @@ struct Vec16;
 template <>
 struct Vec16<double> {
     static constexpr int kVec = 2;
-    __device__ __forceinline__ static uint4 raw(const double *p) { return __ldcs(reinterpret_cast<const uint4 *>(p)); }
+    __device__ __forceinline__ static uint4 raw(const double *p, int64_t) {
+        return __ldcs(reinterpret_cast<const uint4 *>(p));
+    }
     template <typename ACC>
     __device__ __forceinline__ static void get(const uint4 &t, ACC *v) {
         v[0] = (ACC)__hiloint2double((int)t.y, (int)t.x);
@@ -42,7 +44,9 @@ struct Vec16<double> {
 template <>
 struct Vec16<float> {
     static constexpr int kVec = 4;
-    __device__ __forceinline__ static uint4 raw(const float *p) { return __ldcs(reinterpret_cast<const uint4 *>(p)); }
+    __device__ __forceinline__ static uint4 raw(const float *p, int64_t) {
+        return __ldcs(reinterpret_cast<const uint4 *>(p));
+    }
     template <typename ACC>
     __device__ __forceinline__ static void get(const uint4 &t, ACC *v) {
         v[0] = (ACC)__uint_as_float(t.x);
@@ -54,7 +58,7 @@ struct Vec16<float> {
 template <>
 struct Vec16<__nv_bfloat16> {
     static constexpr int kVec = 8;
-    __device__ __forceinline__ static uint4 raw(const __nv_bfloat16 *p) {
+    __device__ __forceinline__ static uint4 raw(const __nv_bfloat16 *p, int64_t) {
         return __ldcs(reinterpret_cast<const uint4 *>(p));
     }
     template <typename ACC>
@@ -66,6 +70,25 @@ struct Vec16<__nv_bfloat16> {
             v[2 * k] = (ACC)__uint_as_float(w[k] << 16);
             v[2 * k + 1] = (ACC)__uint_as_float(w[k] & 0xffff0000u);
         }
+    }
+};
+
+// split FP32 storage: 8 bytes of each plane per thread and column (4 rows);
+// the FP32 words are rebuilt after all loads of a column group are issued
+template <>
+struct Vec16<SplitF32> {
+    static constexpr int kVec = 4;
+    __device__ __forceinline__ static uint4 raw(const SplitF32 *p, int64_t plane) {
+        const uint2 h = __ldcs(reinterpret_cast<const uint2 *>(p));
+        const uint2 l = __ldcs(reinterpret_cast<const uint2 *>(p + plane));
+        return make_uint4(h.x, h.y, l.x, l.y);
+    }
+    template <typename ACC>
+    __device__ __forceinline__ static void get(const uint4 &t, ACC *v) {
+        v[0] = (ACC)__uint_as_float(split_join(t.x & 0xffffu, t.z & 0xffffu));
+        v[1] = (ACC)__uint_as_float(split_join(t.x >> 16, t.z >> 16));
+        v[2] = (ACC)__uint_as_float(split_join(t.y & 0xffffu, t.w & 0xffffu));
+        v[3] = (ACC)__uint_as_float(split_join(t.y >> 16, t.w >> 16));
     }
 };
 
@@ -84,7 +107,8 @@ template <typename S, typename X, typename ACC>
 __global__ void __launch_bounds__(kGemvThreads, GemvMinBlocks<ACC>::value) gemv_partial_kernel(const S *__restrict__ A, int64_t lda, int64_t m,
                                                                     int64_t k, const X *__restrict__ x,
                                                                     int64_t cols_per_split, ACC *__restrict__ work,
-                                                                    int64_t mpad, const int *__restrict__ stop) {
+                                                                    int64_t mpad, const int *__restrict__ stop,
+                                                                    int64_t plane) {
     if (stop && *stop) return;  // a speculatively queued product of a finished solve
     constexpr int VEC = Vec16<S>::kVec;
     const int64_t row = ((int64_t)blockIdx.x * kGemvThreads + threadIdx.x) * VEC;
@@ -100,7 +124,7 @@ __global__ void __launch_bounds__(kGemvThreads, GemvMinBlocks<ACC>::value) gemv_
             uint4 raw[kGemvUnroll];
             ACC xv[kGemvUnroll];
 #pragma unroll
-            for (int u = 0; u < kGemvUnroll; ++u) raw[u] = Vec16<S>::raw(p + (int64_t)u * lda);
+            for (int u = 0; u < kGemvUnroll; ++u) raw[u] = Vec16<S>::raw(p + (int64_t)u * lda, plane);
 #pragma unroll
             for (int u = 0; u < kGemvUnroll; ++u) xv[u] = (ACC)__ldg(x + c + u);
 #pragma unroll
@@ -114,7 +138,7 @@ __global__ void __launch_bounds__(kGemvThreads, GemvMinBlocks<ACC>::value) gemv_
         }
         for (; c < c1; ++c) {
             ACC a[VEC];
-            Vec16<S>::get(Vec16<S>::raw(p), a);
+            Vec16<S>::get(Vec16<S>::raw(p, plane), a);
             const ACC xv = (ACC)__ldg(x + c);
 #pragma unroll
             for (int v = 0; v < VEC; ++v) acc[v] += a[v] * xv;
@@ -183,15 +207,17 @@ int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes) {
     // the largest split buffer over the instances that read elements of this size
     if (elem_bytes == 8) return gemv_work_elems_of<double, double, double>(m, sm_count);
     if (elem_bytes == 4)
-        return std::max(gemv_work_elems_of<float, double, double>(m, sm_count),
-                        gemv_work_elems_of<float, float, float>(m, sm_count));
+        return std::max({gemv_work_elems_of<float, double, double>(m, sm_count),
+                         gemv_work_elems_of<float, float, float>(m, sm_count),
+                         gemv_work_elems_of<SplitF32, double, double>(m, sm_count),
+                         gemv_work_elems_of<SplitF32, float, float>(m, sm_count)});
     return std::max(gemv_work_elems_of<__nv_bfloat16, float, float>(m, sm_count),
                     gemv_work_elems_of<__nv_bfloat16, double, double>(m, sm_count));
 }
 
 template <typename S, typename X, typename ACC, typename Y>
 cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *x, Y *y, const Y *r, ACC *work,
-                        int64_t work_elems, int sm_count, cudaStream_t st, const int *stop) {
+                        int64_t work_elems, int sm_count, cudaStream_t st, const int *stop, int64_t plane) {
     constexpr int VEC = Vec16<S>::kVec;
     const int64_t tiles = (lda + (int64_t)kGemvThreads * VEC - 1) / ((int64_t)kGemvThreads * VEC);
     const int64_t mpad = tiles * kGemvThreads * VEC;
@@ -200,7 +226,7 @@ cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *
     if ((int64_t)splits * mpad > work_elems) return cudaErrorInvalidValue;
     const int64_t cps = (k + splits - 1) / splits;
     dim3 grid((unsigned)tiles, (unsigned)splits);
-    gemv_partial_kernel<S, X, ACC><<<grid, kGemvThreads, 0, st>>>(A, lda, m, k, x, cps, work, mpad, stop);
+    gemv_partial_kernel<S, X, ACC><<<grid, kGemvThreads, 0, st>>>(A, lda, m, k, x, cps, work, mpad, stop, plane);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     gemv_reduce_kernel<ACC, Y><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(work, splits, mpad, m, y, r, stop);
@@ -209,21 +235,28 @@ cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *
 
 template cudaError_t launch_gemv<double, double, double, double>(const double *, int64_t, int64_t, int64_t,
                                                                  const double *, double *, const double *,
-                                                                 double *, int64_t, int, cudaStream_t, const int *);
+                                                                 double *, int64_t, int, cudaStream_t, const int *, int64_t);
 template cudaError_t launch_gemv<float, double, double, double>(const float *, int64_t, int64_t, int64_t,
                                                                 const double *, double *, const double *,
-                                                                double *, int64_t, int, cudaStream_t, const int *);
+                                                                double *, int64_t, int, cudaStream_t, const int *, int64_t);
 template cudaError_t launch_gemv<float, float, float, float>(const float *, int64_t, int64_t, int64_t,
                                                              const float *, float *, const float *, float *,
-                                                             int64_t, int, cudaStream_t, const int *);
+                                                             int64_t, int, cudaStream_t, const int *, int64_t);
 template cudaError_t launch_gemv<__nv_bfloat16, float, float, float>(const __nv_bfloat16 *, int64_t, int64_t,
                                                                      int64_t, const float *, float *,
                                                                      const float *, float *, int64_t, int,
-                                                                     cudaStream_t, const int *);
+                                                                     cudaStream_t, const int *, int64_t);
 template cudaError_t launch_gemv<__nv_bfloat16, double, double, double>(const __nv_bfloat16 *, int64_t, int64_t,
                                                                         int64_t, const double *, double *,
                                                                         const double *, double *, int64_t, int,
-                                                                        cudaStream_t, const int *);
+                                                                        cudaStream_t, const int *, int64_t);
+template cudaError_t launch_gemv<SplitF32, double, double, double>(const SplitF32 *, int64_t, int64_t, int64_t,
+                                                                   const double *, double *, const double *,
+                                                                   double *, int64_t, int, cudaStream_t, const int *,
+                                                                   int64_t);
+template cudaError_t launch_gemv<SplitF32, float, float, float>(const SplitF32 *, int64_t, int64_t, int64_t,
+                                                                const float *, float *, const float *, float *,
+                                                                int64_t, int, cudaStream_t, const int *, int64_t);
 
 // ---------------------------------------------------------------------------
 // reductions
@@ -383,11 +416,11 @@ __global__ void convert_kernel(int64_t n, const TI *x, TO *y) {
 // of a row block of a column-major matrix in any storage precision)
 template <typename T>
 __global__ void gather_rows_kernel(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols,
-                                   double *out) {
+                                   double *out, int64_t plane) {
     const int64_t tot = rows * cols;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t c = e / rows, r = e - c * rows;
-        out[e] = (double)A[row0 + r + c * lda];
+        out[e] = load_entry<T>(A, row0 + r + c * lda, plane);
     }
 }
 
@@ -514,8 +547,8 @@ cudaError_t launch_convert(int64_t n, const TI *x, TO *y, cudaStream_t st) {
 }
 template <typename T>
 cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols, double *out,
-                               cudaStream_t st) {
-    gather_rows_kernel<T><<<grid_for(rows * cols), 256, 0, st>>>(A, lda, row0, rows, cols, out);
+                               cudaStream_t st, int64_t plane) {
+    gather_rows_kernel<T><<<grid_for(rows * cols), 256, 0, st>>>(A, lda, row0, rows, cols, out, plane);
     return cudaGetLastError();
 }
 template <typename T>
@@ -554,11 +587,13 @@ template cudaError_t launch_convert<double, float>(int64_t, const float *, doubl
 template cudaError_t launch_convert<double, __nv_bfloat16>(int64_t, const __nv_bfloat16 *, double *,
                                                            cudaStream_t);
 template cudaError_t launch_gather_rows<double>(const double *, int64_t, int64_t, int64_t, int64_t, double *,
-                                                cudaStream_t);
+                                                cudaStream_t, int64_t);
 template cudaError_t launch_gather_rows<float>(const float *, int64_t, int64_t, int64_t, int64_t, double *,
-                                               cudaStream_t);
+                                               cudaStream_t, int64_t);
 template cudaError_t launch_gather_rows<__nv_bfloat16>(const __nv_bfloat16 *, int64_t, int64_t, int64_t, int64_t,
-                                                       double *, cudaStream_t);
+                                                       double *, cudaStream_t, int64_t);
+template cudaError_t launch_gather_rows<SplitF32>(const SplitF32 *, int64_t, int64_t, int64_t, int64_t, double *,
+                                                  cudaStream_t, int64_t);
 template cudaError_t launch_pair_apply<double>(int, int, int, int, const float *, const int *, int, double,
                                                const double *, double *, cudaStream_t, const int *);
 template cudaError_t launch_pair_apply<float>(int, int, int, int, const float *, const int *, int, double,

@@ -118,8 +118,9 @@ __global__ void __launch_bounds__(kKnnWarps * 32) knn_kernel(int M, const double
 // the couplings B_{i,m} (out[i][m], row-major nb x nb; zero for m >= kp).
 template <typename T>
 __global__ void __launch_bounds__(256) cluster_rows_kernel(int M, int nb, const T *__restrict__ A, int64_t lda,
-                                                           const int *__restrict__ knn, int kstride, int kc, int kp,
-                                                           float *__restrict__ out, int *__restrict__ singular) {
+                                                           int64_t plane, const int *__restrict__ knn, int kstride,
+                                                           int kc, int kp, float *__restrict__ out,
+                                                           int *__restrict__ singular) {
     extern __shared__ float sm[];
     __shared__ int s_fib[32];
     __shared__ int s_piv;
@@ -137,7 +138,7 @@ __global__ void __launch_bounds__(256) cluster_rows_kernel(int M, int nb, const 
         const int r = idx / s, c = idx - r * s;
         const int64_t gr = (int64_t)s_fib[c / nb] * nb + c % nb;
         const int64_t gc = (int64_t)s_fib[r / nb] * nb + r % nb;
-        sm[r * ld + c] = (float)A[gc * lda + gr];
+        sm[r * ld + c] = (float)load_entry<T>(A, gc * lda + gr, plane);
     }
     for (int idx = tid; idx < s * nb; idx += nt) {
         const int r = idx / nb, j = idx - r * nb;
@@ -570,13 +571,20 @@ rf_status build_preconditioner(rf_handle *h) {
             e = cudaFuncSetAttribute(cluster_rows_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
             if (e == cudaSuccess)
-                cluster_rows_kernel<double><<<M, 256, smem, st>>>(M, nb, h->A64, h->lda, h->knn, kK, kc, kp,
+                cluster_rows_kernel<double><<<M, 256, smem, st>>>(M, nb, h->A64, h->lda, 0, h->knn, kK, kc, kp,
                                                                   h->Pblocks, sing);
+        } else if (h->A16lo) {
+            e = cudaFuncSetAttribute(cluster_rows_kernel<SplitF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+            if (e == cudaSuccess)
+                cluster_rows_kernel<SplitF32><<<M, 256, smem, st>>>(
+                    M, nb, reinterpret_cast<const SplitF32 *>(h->A16), h->lda, h->a_plane, h->knn, kK, kc, kp,
+                    h->Pblocks, sing);
         } else {
             e = cudaFuncSetAttribute(cluster_rows_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
             if (e == cudaSuccess)
-                cluster_rows_kernel<float><<<M, 256, smem, st>>>(M, nb, h->A32, h->lda, h->knn, kK, kc, kp,
+                cluster_rows_kernel<float><<<M, 256, smem, st>>>(M, nb, h->A32, h->lda, 0, h->knn, kK, kc, kp,
                                                                  h->Pblocks, sing);
         }
         h->launches++;

@@ -15,6 +15,38 @@ namespace rf {
 constexpr int kPModeFP64 = 0;   // FP64 arithmetic throughout
 constexpr int kPModeMixed = 1;  // FP32 far field, FP64 near field, FP32 projections
 
+// Split storage of the FP32 matrix (mixed BF16 path): two 16-bit planes of
+// lda x n entries each, the high plane first.  The high plane is the BF16
+// matrix of the inner solves: the top 16 bits of each FP32 encoding plus
+// bit 15 (round half away from zero on the bit pattern).  The low plane
+// (`plane` entries further) holds the bottom 16 bits, from which the FP32
+// value is rebuilt exactly: top = high - (low >> 15).  4 bytes per entry
+// instead of 6 for separate FP32 and BF16 matrices.
+struct SplitF32 {
+    unsigned short bits;  // an entry of the high plane
+};
+__host__ __device__ __forceinline__ unsigned short split_hi(unsigned u) {
+    return (unsigned short)((u >> 16) + ((u >> 15) & 1u));
+}
+__host__ __device__ __forceinline__ unsigned split_join(unsigned hi, unsigned lo) {
+    return ((hi - (lo >> 15)) << 16) | lo;
+}
+__device__ __forceinline__ void split_store(float v, __nv_bfloat16 *hi, unsigned short *lo) {
+    const unsigned u = __float_as_uint(v);
+    *reinterpret_cast<unsigned short *>(hi) = split_hi(u);
+    *lo = (unsigned short)(u & 0xffffu);
+}
+// one entry of a matrix stored as T (SplitF32: the planes `plane` apart)
+template <typename T>
+__device__ __forceinline__ double load_entry(const T *A, int64_t idx, int64_t) {
+    return (double)A[idx];
+}
+template <>
+__device__ __forceinline__ double load_entry<SplitF32>(const SplitF32 *A, int64_t idx, int64_t plane) {
+    const unsigned hi = A[idx].bits, lo = A[idx + plane].bits;
+    return (double)__uint_as_float(split_join(hi, lo));
+}
+
 struct AsmArgs {
     int M, N, LQ;
     int t0, t1;                // target fibers [t0, t1) (a row-block shard; 0, M for the whole system)
@@ -23,7 +55,8 @@ struct AsmArgs {
     const Tables *tab;         // device tables
     double *A64;               // FP64 matrix or null
     float *A32;                // FP32 matrix or null
-    __nv_bfloat16 *A16;        // BF16 matrix or null
+    __nv_bfloat16 *A16;        // BF16 matrix (the high plane of split storage) or null
+    unsigned short *A16lo;     // split storage: the low plane, or null
     int64_t lda;
     double *bpart;             // [nchunks][n] partial right-hand sides
     double *PV64, *PW64;       // velocity panels (3M x n, ld ldp) or null
@@ -43,7 +76,8 @@ struct SplitArgs {
     const double *pos, *ori;
     const Tables *tab;
     float *A32;                // FP32 matrix or null
-    __nv_bfloat16 *A16;        // BF16 matrix or null
+    __nv_bfloat16 *A16;        // BF16 matrix (the high plane of split storage) or null
+    unsigned short *A16lo;     // split storage: the low plane, or null
     int64_t lda;
     float *PV32, *PW32;        // velocity panels or null
     int64_t ldp;
@@ -122,9 +156,11 @@ cudaError_t launch_normalize(int M, double *T, cudaStream_t st);
 // mode 0: y = A x;  mode 1: y = r - A x (residual, r given)
 // stop (optional, device): when *stop != 0 at launch time every CTA returns at
 // once (a product queued ahead for a solve that has finished meanwhile).
+// S = SplitF32: A is the high plane, the low plane `plane` entries further.
 template <typename S, typename X, typename ACC, typename Y>
 cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *x, Y *y, const Y *r,
-                        ACC *work, int64_t work_elems, int sm_count, cudaStream_t st, const int *stop = nullptr);
+                        ACC *work, int64_t work_elems, int sm_count, cudaStream_t st, const int *stop = nullptr,
+                        int64_t plane = 0);
 int64_t gemv_work_elems(int64_t m, int sm_count, int elem_bytes);
 
 // ---- Krylov vector kernels ----------------------------------------------------
@@ -181,7 +217,7 @@ cudaError_t launch_convert(int64_t n, const TI *x, TO *y, cudaStream_t st);
 // FP64 copy of rows [row0, row0 + rows) of a column-major matrix (cols columns)
 template <typename T>
 cudaError_t launch_gather_rows(const T *A, int64_t lda, int64_t row0, int64_t rows, int64_t cols, double *out,
-                               cudaStream_t st);
+                               cudaStream_t st, int64_t plane = 0);
 
 // ---- neighbour-block preconditioner (FP32 blocks) -----------------------------
 // z_i = v_i + omega sum_{m < kp} B[i][m] v_{knn[i][m]}, B[i][m] row-major
