@@ -644,3 +644,31 @@ def test_config_matrix_rows_split_kernel_match_oracle(cfg):
             # entry of b, as for A
             eb = np.abs(b[i0 * n3:i1 * n3] - b_o).max() / np.abs(b).max()
             assert eb <= 1e-6, (cfg, i0, eb)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["cloud", "uniform"])
+def test_split_storage_rebuilds_the_fp32_matrix_exactly(kind):
+    """The BF16 path stores its FP32 matrix as two 16-bit planes.  The FP32
+    entries rebuilt from them equal, bit for bit, those the FP32 mixed path
+    stores as FP32 words (the same assembly kernels), and the high plane is
+    the top half of each FP32 word rounded half away from zero."""
+    M = 600
+    if kind == "cloud":
+        pos, ori = rf.generate_layout(M, "gaussian", 3.0 * (M / 4000) ** (1 / 3), 0.2, seed=1720)
+    else:
+        pos, ori = rf.generate_layout(M, "uniform", 4.0, 0.2, seed=1721)
+    rows = {}
+    for prec in (rf.PREC_MIXED_BF16, rf.PREC_MIXED_FP32):
+        p = rf.FiberParams(slenderness=1e-3, precision=prec, velocity_mode=rf.VEL_REUSE)
+        with rf.Simulation(rf.Configuration(p, pos, ori)) as sim:
+            sim.assemble_system()
+            n = sim.n
+            rows[prec] = [sim.matrix_rows(r0, 45) for r0 in (0, n // 2 - 45, n - 45)]
+            if prec == rf.PREC_MIXED_BF16:
+                hi = [sim.matrix_rows(r0, 45, inner=True) for r0 in (0, n // 2 - 45, n - 45)]
+    for a, b, h in zip(rows[rf.PREC_MIXED_BF16], rows[rf.PREC_MIXED_FP32], hi):
+        assert np.array_equal(a, b)
+        u = a.astype(np.float32).view(np.uint32)
+        want = ((u + np.uint32(0x8000)) >> np.uint32(16)).astype(np.uint32) << np.uint32(16)
+        assert np.array_equal(h.astype(np.float32).view(np.uint32), want)
