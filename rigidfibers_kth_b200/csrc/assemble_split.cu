@@ -3,7 +3,9 @@
 // Reference: fortran/matrix_assembly.f90:407-629 (matrix, analytic) and
 // 796-905 (right-hand side); Int_analytical.f90:72-288 (inner integral).
 //
-// The mixed path stores A in FP32 (and BF16).  A fiber pair (i, j) is "near"
+// The mixed path stores A in FP32: as FP32 words (FP32 paths) or as the two
+// 16-bit planes of split storage (BF16 path; the high plane is the BF16
+// matrix of the inner solves).  A fiber pair (i, j) is "near"
 // when one of target i's quadrature points lies within sqrt(near_c) of source
 // j's centre (default c < 6: closer, the FP32 backward recursion loses digits;
 // the reference itself switches to forward recursion below 10).  Near pairs
@@ -17,9 +19,10 @@
 //                     warps per CTA stepping through the sources together:
 //                     every lane integrates its own pair over the target's
 //                     Gauss points with the projection accumulated in
-//                     registers, then stages the 3N x 3N block (and its BF16
-//                     copy and the velocity-panel rows) in shared memory and
-//                     one lane hands whole column segments to the copy engine;
+//                     registers, then stages the 3N x 3N block (split into
+//                     its two 16-bit planes where stored so) and the
+//                     velocity-panel rows in shared memory, and one lane
+//                     hands whole column segments to the copy engine;
 //   near_pairs_kernel FP64, one warp per near pair: lane = Gauss point, the
 //                     projection on the FP64 tensor cores (mma.sync m8n8k4).
 // A finish kernel sums the per-chunk right-hand-side partials in a fixed order.
@@ -325,9 +328,10 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
     const int nrows = nvalid * RB;
     const int64_t col0 = (int64_t)j * RB + 3 * (m - 1);
     if (nrows == GR) {
-        // whole column segments: the BF16 copy is staged too, then one lane
-        // hands every segment to the copy engine (A32 and A16: 3 x 32 targets
-        // x 3N rows; panels: 2 x 3 x 96 rows), and the warp moves on
+        // whole column segments: the 16-bit planes (or the BF16 copy) are
+        // staged too, then one lane hands every segment to the copy engine
+        // (the matrix: 3 x 32 targets x 3N rows; panels: 2 x 3 x 96 rows),
+        // and the warp moves on
         if (a.A16lo) {
             // split FP32 storage: the low plane goes to the BF16 staging, the
             // high plane over the first half of the FP32 staging it is read
