@@ -54,6 +54,7 @@ struct SplitDims {
     static constexpr int NL = N + 1;          // u_p and Legendre indices 0..N
     static constexpr int NV = N + 3;          // v_p, p = 0..N+2
     static constexpr int KW = N + 3;          // projection rows k = 0..N+2
+    static constexpr int KWP = KW + (KW & 1); // KW rounded up to even: the weight table's row stride
     static constexpr int NC = NL + NV;        // scalars per Gauss point
     static constexpr int RB = 3 * N;          // rows (and columns) of a pair block
     static constexpr int NRHS = 3 * NL;       // theta^k_0 f, k = 0..N
@@ -293,7 +294,7 @@ struct FarSmem {
     static constexpr int PAN = 2 * 3 * 96;                  // staged panel columns
     static constexpr int STG16 = 3 * GR / 2;                // BF16 copy (split storage: low plane) of the staged columns
     static constexpr size_t kBytes = sizeof(float) * (32 * kNearWeight + 16 + 64 + kMaxLQ +
-                                                      kMaxLQ * SplitDims<N>::KW + 3 * GR + (PANELS ? PAN : 0) +
+                                                      kMaxLQ * SplitDims<N>::KWP + 3 * GR + (PANELS ? PAN : 0) +
                                                       STG16);
     static_assert(kBytes % 16 == 0, "each warp's region starts on a 16-byte boundary");
     static size_t bytes() { return kBytes; }
@@ -488,17 +489,17 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
     int *s_nl = reinterpret_cast<int *>(s_gk + 16);                   // near lanes of the source, in order
     int *s_ns = s_nl + 32;                                            // and their buffer slots
     float *s_pv = reinterpret_cast<float *>(s_ns + 32);
-    float *s_w = s_pv + kMaxLQ;                                       // [kMaxLQ][KW]: w_q P_k(s_q)
-    float *s_stg = s_w + kMaxLQ * KW;                                 // [3][GR]
+    float *s_w = s_pv + kMaxLQ;                                       // [kMaxLQ][KWP]: w_q P_k(s_q), k >= KW zero
+    float *s_stg = s_w + kMaxLQ * SD::KWP;                            // [3][GR]
     float *s_pan = s_stg + 3 * GR;                                    // [2][3][96]
     __nv_bfloat16 *s_stg16 = reinterpret_cast<__nv_bfloat16 *>(s_pan + (PANELS ? SM::PAN : 0));  // [3][GR]
 
     const Tables &tab = *a.tab;
     const int LQ = a.LQ;
     for (int t = lane; t < kMaxLQ; t += 32) s_pv[t] = t < LQ ? (float)tab.pv[t] : 0.f;
-    for (int t = lane; t < kMaxLQ * KW; t += 32) {
-        const int q = t / KW, k = t - q * KW;
-        s_w[t] = q < LQ ? (float)(tab.wv[q] * tab.P[k][q]) : 0.f;
+    for (int t = lane; t < kMaxLQ * SD::KWP; t += 32) {
+        const int q = t / SD::KWP, k = t - q * SD::KWP;
+        s_w[t] = (q < LQ && k < KW) ? (float)(tab.wv[q] * tab.P[k][q]) : 0.f;
     }
     if (lane < 8) {
         s_gk[lane] = lane <= N ? (float)tab.gamma[lane] : 0.f;
@@ -586,23 +587,40 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
 #pragma unroll
             for (int k = 0; k < KW; ++k) V[pp][k] = 0.f;
         // the Gauss point q's moments, weighted, into the projections
+        // Pairs of rows (k, k + 1) go through the packed FP32 units: each half
+        // of __ffma2_rn is the fmaf of the scalar form, so the sums are the same.
         auto add_point = [&](int q, const float *I, const float *J, const float *S) {
-            const float *w = s_w + q * KW;
-            float wk[KW];
+            constexpr int KWP = SD::KWP;
+            const float2 *w2 = reinterpret_cast<const float2 *>(s_w + q * KWP);  // even stride: 8-byte aligned
+            float2 wk[KWP / 2];
 #pragma unroll
-            for (int k = 0; k < KW; ++k) wk[k] = w[k];
+            for (int k = 0; k < KWP / 2; ++k) wk[k] = w2[k];
 #pragma unroll
             for (int pp = 0; pp < NL; ++pp) {
                 const float u = fmaf(e2, J[pp], I[pp]);
+                const float2 u2 = make_float2(u, u);
 #pragma unroll
-                for (int k = 0; k < NL; ++k) U[pp][k] = fmaf(wk[k], u, U[pp][k]);
+                for (int k = 0; k + 1 < NL; k += 2) {
+                    const float2 r = __ffma2_rn(wk[k / 2], u2, make_float2(U[pp][k], U[pp][k + 1]));
+                    U[pp][k] = r.x;
+                    U[pp][k + 1] = r.y;
+                }
+                if (NL % 2) U[pp][NL - 1] = fmaf(wk[(NL - 1) / 2].x, u, U[pp][NL - 1]);
             }
 #pragma unroll
             for (int pp = 0; pp < NV; ++pp) {
                 const float v = fmaf(-e6, S[pp], J[pp]);
+                const float2 v2 = make_float2(v, v);
 #pragma unroll
-                for (int k = 0; k < KW; ++k)
-                    if (k < vrows(N, pp)) V[pp][k] = fmaf(wk[k], v, V[pp][k]);
+                for (int k = 0; k < KW; k += 2) {
+                    if (k + 1 < vrows(N, pp)) {
+                        const float2 r = __ffma2_rn(wk[k / 2], v2, make_float2(V[pp][k], V[pp][k + 1]));
+                        V[pp][k] = r.x;
+                        V[pp][k + 1] = r.y;
+                    } else if (k < vrows(N, pp)) {
+                        V[pp][k] = fmaf(wk[k / 2].x, v, V[pp][k]);
+                    }
+                }
             }
         };
         if (act) {
