@@ -209,8 +209,9 @@ rf_status rf_get_matrix(rf_handle *h, double *A);
  * column-major (leading dimension rows), for checking a sample of a system
  * too large to copy whole (the reference dumps all of A,
  * src/simulation.cu:468-546).  which = 0: the matrix of the FP64 path or of
- * the refinement residual (FP64 or FP32 storage); which = 1: the matrix of
- * the inner solve (the BF16 copy where there is one, else as 0). */
+ * the refinement residual (FP64 or FP32 storage; RF_PREC_MIXED_BF16: the FP32
+ * entries rebuilt from its two 16-bit planes); which = 1: the matrix of the
+ * inner solve (the BF16 high plane where there is one, else as 0). */
 rf_status rf_get_matrix_rows(rf_handle *h, int32_t which, int64_t row0, int64_t rows, double *out);
 /* y = A x with the stored matrix (FP64 host vectors of n doubles). */
 rf_status rf_matvec(rf_handle *h, const double *x, double *y);
