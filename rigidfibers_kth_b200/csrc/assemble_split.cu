@@ -314,6 +314,8 @@ __device__ __forceinline__ void bulk_s2g(void *gdst, const void *ssrc, unsigned 
                  : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// lanes of a far-pair warp that hand staged column segments to the copy engine
+constexpr int kCopyLanes = 12;
 // the staged data has been read out: the staging buffers may be rewritten
 __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
@@ -367,25 +369,28 @@ __device__ __forceinline__ void far_store_m(const SplitArgs &a, int m, int j, in
         }
         fence_async_shared();
         __syncwarp();
-        if (lane == 0) {
-#pragma unroll
-            for (int bb = 0; bb < 3; ++bb) {
-                const int64_t col = col0 + bb;
-                if (a.A32) bulk_s2g(a.A32 + col * a.lda + row0, stg + bb * GR, GR * sizeof(float));
-                if (a.A16lo) {
+        // one segment per lane: lane l copies column bb = l % 3 of kind l / 3
+        // (0: the FP32 words or the high plane, 1: the low plane or the BF16
+        // copy, 2 and 3: the two panels); each lane commits its own group
+        if (lane < kCopyLanes) {
+            const int bb = lane % 3, kind = lane / 3;
+            const int64_t col = col0 + bb;
+            if (kind == 0) {
+                if (a.A32)
+                    bulk_s2g(a.A32 + col * a.lda + row0, stg + bb * GR, GR * sizeof(float));
+                else if (a.A16lo)
                     bulk_s2g(a.A16 + col * a.lda + row0, reinterpret_cast<const unsigned short *>(stg) + bb * GR,
                              GR * sizeof(unsigned short));
+            } else if (kind == 1) {
+                if (a.A16lo)
                     bulk_s2g(a.A16lo + col * a.lda + row0, reinterpret_cast<const unsigned short *>(stg16) + bb * GR,
                              GR * sizeof(unsigned short));
-                } else if (a.A16) {
+                else if (a.A16)
                     bulk_s2g(a.A16 + col * a.lda + row0, stg16 + bb * GR, GR * sizeof(__nv_bfloat16));
-                }
-                if (PANELS) {
-#pragma unroll
-                    for (int w = 0; w < 2; ++w)
-                        bulk_s2g((w ? a.PW32 : a.PV32) + col * a.ldp + (int64_t)i0 * 3, pan + (w * 3 + bb) * 96,
-                                 96 * sizeof(float));
-                }
+            } else if (PANELS) {
+                const int w = kind - 2;
+                bulk_s2g((w ? a.PW32 : a.PV32) + col * a.ldp + (int64_t)i0 * 3, pan + (w * 3 + bb) * 96,
+                         96 * sizeof(float));
             }
             bulk_commit();
         }
@@ -704,7 +709,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
         for (int it = 0; it < N; ++it) {
             const int m = it < (N + 1) / 2 ? 2 * it + 1 : 2 * (it - (N + 1) / 2) + 2;
             // the copy engine has read the previous weight's staged columns
-            if (lane == 0) bulk_wait_read();
+            if (lane < kCopyLanes) bulk_wait_read();
             __syncwarp();
             float S[7][N + 1];
             if (m & 1) far_sets_reg<N, 1>(m, U, V, S);
@@ -791,7 +796,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
 #pragma unroll
         for (int r = 0; r < NRHS; ++r) a.far_contr[((int64_t)blockIdx.y * a.M + i) * NRHS + r] = rhs[r];
     }
-    if (lane == 0) bulk_wait_all();  // every staged segment written before the CTA's shared memory goes
+    if (lane < kCopyLanes) bulk_wait_all();  // every staged segment written before the CTA's shared memory goes
 }
 
 // ---------------------------------------------------------------- near pairs (FP64)
