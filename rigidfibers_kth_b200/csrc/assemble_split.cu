@@ -467,16 +467,52 @@ __device__ __forceinline__ void far_sets_reg(int m, const float (&U)[N + 1][N + 
     }
 }
 
+// A 3-vector with components 0 and 1 packed for the paired FP32 units.
+struct V3p {
+    float2 xy;
+    float z;
+};
+__device__ __forceinline__ V3p v3p(const float *v) { return {make_float2(v[0], v[1]), v[2]}; }
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+// a A + b B + c C
+__device__ __forceinline__ V3p comb3(float a, const V3p &A, float b, const V3p &B, float c, const V3p &C) {
+    V3p r;
+    r.xy = __ffma2_rn(dup2(c), C.xy, __ffma2_rn(dup2(b), B.xy, __fmul2_rn(dup2(a), A.xy)));
+    r.z = fmaf(c, C.z, fmaf(b, B.z, a * A.z));
+    return r;
+}
+// a A + b B + c C + d E
+__device__ __forceinline__ V3p comb4(float a, const V3p &A, float b, const V3p &B, float c, const V3p &C, float d,
+                                     const V3p &E) {
+    V3p r;
+    r.xy = __ffma2_rn(dup2(d), E.xy,
+                      __ffma2_rn(dup2(c), C.xy, __ffma2_rn(dup2(b), B.xy, __fmul2_rn(dup2(a), A.xy))));
+    r.z = fmaf(d, E.z, fmaf(c, C.z, fmaf(b, B.z, a * A.z)));
+    return r;
+}
+
 // X = R0 D + R1 t + C0 p, Y = R1 D + R2 t + C1 p, Z = C0 D + C1 t + E p for row k
 template <int N>
-__device__ __forceinline__ void far_xyz_r(const float (&S)[7][N + 1], int k, const float *D, const float *t,
-                                          const float *p, float *X, float *Y, float *Z) {
+__device__ __forceinline__ void far_xyz_p(const float (&S)[7][N + 1], int k, const V3p &D, const V3p &t,
+                                          const V3p &p, V3p &X, V3p &Y, V3p &Z) {
     const float R0 = S[1][k], R1 = S[2][k], R2 = S[3][k], C0 = S[4][k], C1 = S[5][k], E = S[6][k];
+    X = comb3(R0, D, R1, t, C0, p);
+    Y = comb3(R1, D, R2, t, C1, p);
+    Z = comb3(C0, D, C1, t, E, p);
+}
+
+// The 3 x 3 entries sc (AI delta_ab + D_a X_b + t_a Y_b + p_a Z_b) at
+// dst[b * ld + a]; columns b = 0, 1 as a packed pair.
+__device__ __forceinline__ void block3(float *dst, int ld, float sc, float AI, const float *D, const float *t,
+                                       const float *p, const V3p &X, const V3p &Y, const V3p &Z) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        X[c] = R0 * D[c] + R1 * t[c] + C0 * p[c];
-        Y[c] = R1 * D[c] + R2 * t[c] + C1 * p[c];
-        Z[c] = C0 * D[c] + C1 * t[c] + E * p[c];
+    for (int a = 0; a < 3; ++a) {
+        const float2 d0 = make_float2(a == 0 ? AI : 0.f, a == 1 ? AI : 0.f);
+        float2 e = __ffma2_rn(dup2(p[a]), Z.xy, __ffma2_rn(dup2(t[a]), Y.xy, __ffma2_rn(dup2(D[a]), X.xy, d0)));
+        e = __fmul2_rn(dup2(sc), e);
+        dst[a] = e.x;
+        dst[ld + a] = e.y;
+        dst[2 * ld + a] = sc * fmaf(p[a], Z.z, fmaf(t[a], Y.z, fmaf(D[a], X.z, a == 2 ? AI : 0.f)));
     }
 }
 
@@ -714,52 +750,44 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
             float S[7][N + 1];
             if (m & 1) far_sets_reg<N, 1>(m, U, V, S);
             else far_sets_reg<N, 0>(m, U, V, S);
+            // the block entries and panel rows: theta's 3 x 3 blocks with their
+            // columns (components of X, Y, Z) paired on the packed FP32 units
+            const V3p Dp = v3p(D), tp = v3p(t), pp3 = v3p(p);
             // row k = 0: velocity panel P0 only
             if (PANELS) {
-                float X[3], Y[3], Z[3];
-                far_xyz_r<N>(S, 0, D, t, p, X, Y, Z);
-                const float AI = S[0][0];
-#pragma unroll
-                for (int bb = 0; bb < 3; ++bb)
-#pragma unroll
-                    for (int aa = 0; aa < 3; ++aa)
-                        s_pan[bb * 96 + lane * 3 + aa] =
-                            sv * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * Y[bb] + p[aa] * Z[bb]);
+                V3p X, Y, Z;
+                far_xyz_p<N>(S, 0, Dp, tp, pp3, X, Y, Z);
+                block3(s_pan + lane * 3, 96, sv, S[0][0], D, t, p, X, Y, Z);
             }
             // row k = 1: block row D1 t (theta t)^T and velocity panel P1
             {
-                float X[3], Y[3], Z[3], Q[3];
-                far_xyz_r<N>(S, 1, D, t, p, X, Y, Z);
+                V3p X, Y, Z;
+                far_xyz_p<N>(S, 1, Dp, tp, pp3, X, Y, Z);
                 const float AI = S[0][1];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) Q[c] = AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c];
+                const V3p Q = comb4(AI, tp, Dt, X, tt, Y, pt, Z);
+                const float Qv[3] = {Q.xy.x, Q.xy.y, Q.z};
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
-                    for (int aa = 0; aa < 3; ++aa) s_stg[bb * GR + lane * RB + aa] = D1 * t[aa] * Q[bb];
+                    for (int aa = 0; aa < 3; ++aa) s_stg[bb * GR + lane * RB + aa] = D1 * t[aa] * Qv[bb];
                 if (PANELS) {
-#pragma unroll
-                    for (int bb = 0; bb < 3; ++bb)
-#pragma unroll
-                        for (int aa = 0; aa < 3; ++aa)
-                            s_pan[(3 + bb) * 96 + lane * 3 + aa] =
-                                sw * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * (Y[bb] - Q[bb]) + p[aa] * Z[bb]);
+                    V3p YQ;
+                    YQ.xy = make_float2(Y.xy.x - Q.xy.x, Y.xy.y - Q.xy.y);
+                    YQ.z = Y.z - Q.z;
+                    block3(s_pan + 3 * 96 + lane * 3, 96, sw, AI, D, t, p, X, YQ, Z);
                 }
             }
             // rows k = 2..N: gamma_k (theta - E_k t (theta t)^T)
 #pragma unroll
             for (int k = 2; k <= N; ++k) {
-                float X[3], Y[3], Z[3], W[3];
-                far_xyz_r<N>(S, k, D, t, p, X, Y, Z);
+                V3p X, Y, Z;
+                far_xyz_p<N>(S, k, Dp, tp, pp3, X, Y, Z);
                 const float AI = S[0][k], g = s_gk[k], ek = s_gk[8 + k];
-#pragma unroll
-                for (int c = 0; c < 3; ++c) W[c] = Y[c] - ek * (AI * t[c] + Dt * X[c] + tt * Y[c] + pt * Z[c]);
-                float *dst = s_stg + lane * RB + 3 * (k - 1);
-#pragma unroll
-                for (int bb = 0; bb < 3; ++bb)
-#pragma unroll
-                    for (int aa = 0; aa < 3; ++aa)
-                        dst[bb * GR + aa] = g * ((aa == bb ? AI : 0.f) + D[aa] * X[bb] + t[aa] * W[bb] + p[aa] * Z[bb]);
+                const V3p Q = comb4(AI, tp, Dt, X, tt, Y, pt, Z);
+                V3p W;
+                W.xy = __ffma2_rn(dup2(-ek), Q.xy, Y.xy);
+                W.z = fmaf(-ek, Q.z, Y.z);
+                block3(s_stg + lane * RB + 3 * (k - 1), GR, g, AI, D, t, p, X, W, Z);
             }
             // the diagonal pair (its projections are zero): identity where k = m
             if (diag) {
