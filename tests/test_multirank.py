@@ -108,3 +108,25 @@ def test_reference_arm_loads_only_the_oracle():
     assert r.returncode == 0, r.stderr
     d = json.loads(r.stdout.strip().splitlines()[-1])
     assert d == {"ok": True, "product": False, "oracle": True}
+
+
+def test_reference_gpu_arm_parses_the_programs_timers_and_reports_a_missing_build(monkeypatch):
+    """`bench.py --impl reference-gpu`: the phase times come from the
+    reference program's own "[BENCHMARK]" lines (seconds, last then average);
+    without the built program the arm prints its `unavailable` line."""
+    import bench
+
+    out = ("     [GPU]      : Assembling system...\n"
+           "  [BENCHMARK]   : assemble_system   : 0.00298(0.00298) sec\n"
+           "  [BENCHMARK]   : solve_system      : 0.00653(0.00653) sec\n"
+           "  [BENCHMARK]   : update_velocities : 0.00735(0.00735) sec\n"
+           "  [BENCHMARK]   : update_fibers_firststep : 0.00008(0.00008) sec\n")
+    ph = bench._ref_gpu_phases(out)
+    assert set(ph) == set(bench.REF_GPU_PHASES)
+    assert ph["solve_system"] == 0.00653
+    # the parameter file is the positional v1 format of run100_iter.in
+    assert len(bench.REF_GPU_PARAMS) == 14 and bench.REF_GPU_PARAMS[3] == "0.01"
+    monkeypatch.setattr(bench, "REF_GPU_EXE", os.path.join(ROOT, "oracle", "_ref", "no_such_program"))
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference-gpu", "--steps", "1", "--warmup", "0"])
+    d = bench.run_reference_gpu(bench.parse_args())
+    assert d["impl"] == "reference-gpu" and "unavailable" in d
