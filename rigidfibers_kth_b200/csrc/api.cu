@@ -167,6 +167,7 @@ namespace {
 // Mixed solves that start from zero after a warm start left more than 10 %
 // of |b|; the next one tries the warm start again.
 constexpr int kWarmRetry = 8;
+constexpr int kWarmRetryMax = 64;  // the wait doubles after each poor warm start up to this
 // The block preconditioner is kept only while it pays.  The solver keeps a
 // running mean of the iterations of its solves with and without it; after a
 // solve whose blocks missed a trial (see rf_solve_system), or whose mean is
@@ -900,14 +901,22 @@ rf_status rf_solve_system(rf_handle *h) {
         // sedimenting cloud it leaves 40-70 % of |b| (the near-field
         // couplings change too much in one step), less than one inner
         // iteration saves, and checking it costs an FP32-matrix product.
-        // After a poor warm start the next kWarmRetry solves start from zero.
-        const bool warm = h->cold_solves == 0;
+        // After a poor warm start the next kWarmRetry solves start from zero,
+        // after a second one twice as many, up to kWarmRetryMax; a handle
+        // without a previous solution (none solved or restored yet) starts
+        // from zero without the check.
+        const bool warm = h->x_valid && h->cold_solves == 0;
         if (warm) {
             if (e == cudaSuccess) e = residual();
             if (e == cudaSuccess) e = norm_of(h->r64, &rn);
-            if (e == cudaSuccess && bn > 0.0 && rn > 0.1 * bn) h->cold_solves = kWarmRetry;
+            if (e == cudaSuccess && bn > 0.0 && rn > 0.1 * bn) {
+                h->cold_solves = h->warm_wait;
+                h->warm_wait = std::min(2 * h->warm_wait, kWarmRetryMax);
+            } else {
+                h->warm_wait = kWarmRetry;
+            }
         } else {
-            --h->cold_solves;
+            if (h->cold_solves > 0) --h->cold_solves;
             if (e == cudaSuccess) e = cudaMemsetAsync(h->x, 0, sizeof(double) * h->n, st);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(h->r64, h->b, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, st);
@@ -973,6 +982,7 @@ rf_status rf_solve_system(rf_handle *h) {
             }
         }
         CK(h, e, "mixed-precision solve");
+        h->x_valid = true;
         h->stats.iterations = iters;
         h->stats.refinements = it;
         h->stats.residual = bn > 0.0 ? rn / bn : 0.0;
@@ -1266,7 +1276,10 @@ rf_status rf_set_history(rf_handle *h, const double *prev_pos, const double *pre
     if (prev_orient) CK(h, cudaMemcpy(h->T[h->prev], prev_orient, m3, cudaMemcpyHostToDevice), "upload");
     if (prev_vel) CK(h, cudaMemcpy(h->V[h->vprev], prev_vel, m3, cudaMemcpyHostToDevice), "upload");
     if (prev_rot) CK(h, cudaMemcpy(h->W[h->vprev], prev_rot, m3, cudaMemcpyHostToDevice), "upload");
-    if (coeffs) CK(h, cudaMemcpy(h->x, coeffs, h->n * 8, cudaMemcpyHostToDevice), "upload");
+    if (coeffs) {
+        CK(h, cudaMemcpy(h->x, coeffs, h->n * 8, cudaMemcpyHostToDevice), "upload");
+        h->x_valid = true;
+    }
     return RF_OK;
 }
 

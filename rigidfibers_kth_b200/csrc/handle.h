@@ -116,6 +116,8 @@ struct rf_handle {
 
     rf_solve_stats stats{};
     int cold_solves = 0;  // mixed solves left that start from zero (poor warm start seen)
+    int warm_wait = 8;    // solves to start from zero after the next poor warm start
+    bool x_valid = false; // x holds a solution (solved, or restored by rf_set_history)
     int pc_skips = 0;     // solves left that skip the block preconditioner
     double pc_its[2] = {-1.0, -1.0};  // running mean of solve iterations without / with it (-1: none yet)
     int pc_age = 0;       // preconditioned solves since the last one without it

@@ -471,6 +471,27 @@ def test_not_converged_status_and_state_still_advances(golden):
         assert np.isfinite(P).all()
 
 
+@pytest.mark.parametrize("pc", [rf.PC_NONE, rf.PC_LEARNED])
+def test_mixed_not_converged_status_and_state_still_advances(golden, pc):
+    """The mixed path with a refinement budget too small for the tolerance:
+    the step reports RF_ERR_NOT_CONVERGED with the reached residual, the state
+    still advances, and the next step runs."""
+    import os
+
+    X, T = golden_layout(golden)
+    with make_sim(X, T, gmres_tol=1e-10, precision=rf.PREC_MIXED_BF16, velocity_mode=rf.VEL_REUSE,
+                  max_refinements=1, preconditioner=pc) as sim:
+        if pc == rf.PC_LEARNED:
+            sim.set_mlp_weights(np.load(os.path.join(os.path.dirname(rf.__file__), "mlp_weights.npy")))
+        assert sim.step(0) == 4  # RF_ERR_NOT_CONVERGED
+        s = sim.solve_stats()
+        assert not s["converged"] and s["refinements"] == 1 and 1e-10 < s["residual"] < 1e-2
+        P, _ = sim.state()
+        assert np.isfinite(P).all()
+        assert sim.step(1) == 4
+        assert np.isfinite(sim.state()[0]).all()
+
+
 def test_checkpoint_resume_matches_uninterrupted(golden):
     X, T = golden_layout(golden, 60)
     kw = dict(gmres_tol=1e-10, gmres_max_iters=300)
