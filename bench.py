@@ -102,6 +102,8 @@ def parse_args():
     ap.add_argument("--weights", default=os.path.join(ROOT, "rigidfibers_kth_b200", "mlp_weights.npy"))
     ap.add_argument("--pc-damping", type=float, default=None,
                     help="damping of the preconditioner's coupling blocks (default: the library's)")
+    ap.add_argument("--near-c", type=float, default=None,
+                    help="squared distance below which a pair's integrals stay FP64 (default: the library's)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=4,
@@ -221,6 +223,8 @@ def workload_config(M, world):
 # ---------------------------------------------------------------- product arm
 # block damping (FiberParams.pc_damping) of the preconditioned arms; None: the library's default
 PC_DAMPING = None
+# near-pair threshold (FiberParams.near_field_c) of the mixed arms; None: the library's default
+NEAR_C = None
 
 
 def make_sim(rf, pos, ori, device, precision, pc, velocity_mode, tol=WORKLOAD["tol"]):
@@ -230,6 +234,8 @@ def make_sim(rf, pos, ori, device, precision, pc, velocity_mode, tol=WORKLOAD["t
                        precision=precision, preconditioner=pc, velocity_mode=velocity_mode, device=device)
     if PC_DAMPING is not None:
         p.pc_damping = PC_DAMPING
+    if NEAR_C is not None:
+        p.near_field_c = NEAR_C
     return rf.Simulation(rf.Configuration(p, pos, ori))
 
 
@@ -494,6 +500,7 @@ def run_ours(args):
             "arm": {"precision": args.precision + " A (inner GMRES) + FP32 A (FP64-accumulated residual) + FP64 "
                                  "refinement", "preconditioner": args.pc,
                     "pc_damping": PC_DAMPING if PC_DAMPING is not None else "library default",
+                    "near_field_c": NEAR_C if NEAR_C is not None else "library default",
                     "velocities": "stored P0/P1 projection panels"},
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -535,6 +542,8 @@ def config_sim(rf, cfg, pos, ori, device, precision, tol, pc, velocity_mode):
                        velocity_mode=velocity_mode, device=device)
     if PC_DAMPING is not None:
         p.pc_damping = PC_DAMPING
+    if NEAR_C is not None:
+        p.near_field_c = NEAR_C
     return rf.Simulation(rf.Configuration(p, pos, ori))
 
 
@@ -913,9 +922,10 @@ def run_reference_gpu(args):
 
 
 def main():
-    global PC_DAMPING
+    global PC_DAMPING, NEAR_C
     args = parse_args()
     PC_DAMPING = args.pc_damping
+    NEAR_C = args.near_c
     if args.impl == "reference":
         out = run_reference(args)
     elif args.impl == "reference-gpu":

@@ -1,6 +1,8 @@
 // api.cu - the C ABI (include/rigidfibers.h): handle life cycle and the
 // reference step API (src/simulation.cu:40-424 of the reference):
 // assemble_system -> solve_system -> update_velocities -> update_fibers.
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -50,6 +52,7 @@ void free_all(rf_handle *h) {
                     h->dscal, h->rb.partials, h->rb.counter, h->near_bits, h->near_list, h->near_cnt,
                     h->far_contr, h->near_contr, h->near_pref, h->near_off, h->near_total, h->nearbuf};
     for (void *p : ptrs) cudaFree(p);
+    if (h->blas) cublasDestroy(static_cast<cublasHandle_t>(h->blas));
     h->gm64.reset();
     h->gm32.reset();
     if (h->hscal) cudaFreeHost(h->hscal);
@@ -716,9 +719,16 @@ rf_status rf_solve_system(rf_handle *h) {
             CK(h, cudaMalloc(&h->lu_piv, sizeof(int) * h->n), "direct solver");
             CK(h, cudaMalloc(&h->lu_info, sizeof(int)), "direct solver");
         }
+        if (!h->blas) {
+            cublasHandle_t bh = nullptr;
+            if (cublasCreate(&bh) != CUBLAS_STATUS_SUCCESS)
+                return rf::fail(h, RF_ERR_CUDA, "direct solver: cuBLAS handle could not be created");
+            h->blas = bh;
+        }
         CK(h, cudaMemcpyAsync(h->LU, h->A64, mat, cudaMemcpyDeviceToDevice, st), "direct solver");
         CK(h, cudaMemcpyAsync(h->x, h->b, sizeof(double) * h->n, cudaMemcpyDeviceToDevice, st), "direct solver");
-        CK(h, rf::lu_factor(h->LU, h->lda, h->n, h->lu_piv, h->lu_info, st, &h->launches), "LU factorisation");
+        CK(h, rf::lu_factor(h->LU, h->lda, h->n, h->lu_piv, h->lu_info, h->blas, st, &h->launches),
+           "LU factorisation");
         CK(h, rf::lu_solve(h->LU, h->lda, h->n, h->lu_piv, h->x, st, &h->launches), "LU solve");
         // backward error |b - A x| / |b| for the statistics
         CK(h, (rf::launch_gemv<double, double, double, double>(h->A64, h->lda, h->n, h->n, h->x, h->lu_r, h->b,

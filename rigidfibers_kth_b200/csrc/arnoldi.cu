@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(kThreads) start_kernel(int64_t n, const T *__r
 // out = w / hnext, unless the solve has stopped (or out is not needed)
 template <typename T>
 __global__ void scale_next_kernel(int64_t n, const T *__restrict__ w, T *__restrict__ out, const ArnoldiCtrl *c) {
+    pdl_wait();
     if (c->stop) return;
     const double inv = 1.0 / c->hnext;
     for (int64_t e = (int64_t)blockIdx.x * kThreads + threadIdx.x; e < n; e += (int64_t)gridDim.x * kThreads)
@@ -149,6 +150,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) cgs_dots_kernel(int64_t n, const T *__restrict__ w,
                                                             const T *__restrict__ V, int j1, ArnoldiCtrl *c,
                                                             double *part, unsigned int *counter) {
+    pdl_wait();
     if (c->stop) return;
     double acc[KM];
 #pragma unroll
@@ -174,6 +176,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) cgs_update_dots_kernel(int64_t n, T *__restrict__ w,
                                                                    const T *__restrict__ V, int j1, ArnoldiCtrl *c,
                                                                    double *part, unsigned int *counter) {
+    pdl_wait();
     if (c->stop) return;
     __shared__ double hs[KM];
     if ((int)threadIdx.x < j1) hs[threadIdx.x] = c->h1[threadIdx.x];
@@ -215,6 +218,7 @@ __global__ void __launch_bounds__(kThreads) cgs_update_norm_kernel(int64_t n, T 
                                                                    const T *__restrict__ V, int j, ArnoldiCtrl *c,
                                                                    ArnoldiStat *stat, double *part,
                                                                    unsigned int *counter) {
+    pdl_wait();
     if (c->stop) return;
     const int j1 = j + 1;
     __shared__ double hs[KM];
@@ -312,11 +316,19 @@ cudaError_t launch_arnoldi_orthogonalize(int64_t n, T *w, T *V, int j, int m, Ar
                                          double *part, unsigned int *counter, int max_blocks, cudaStream_t st) {
     if (j < 0 || j >= m || m > KM) return cudaErrorInvalidValue;
     const int nb = blocks_for(n, max_blocks);
-    cgs_dots_kernel<T><<<nb, kThreads, 0, st>>>(n, w, V, j + 1, c, part, counter);
-    cgs_update_dots_kernel<T><<<nb, kThreads, 0, st>>>(n, w, V, j + 1, c, part, counter);
-    cgs_update_norm_kernel<T><<<nb, kThreads, 0, st>>>(n, w, V, j, c, stat, part, counter);
-    if (j + 1 < m) scale_next_kernel<T><<<nb, kThreads, 0, st>>>(n, w, V + (int64_t)(j + 1) * n, c);
-    return cudaGetLastError();
+    // each kernel waits (pdl_wait) for the previous one before touching memory
+    cudaError_t e = launch_pdl(cgs_dots_kernel<T>, dim3(nb), dim3(kThreads), 0, st, n, static_cast<const T *>(w),
+                               static_cast<const T *>(V), j + 1, c, part, counter);
+    if (e == cudaSuccess)
+        e = launch_pdl(cgs_update_dots_kernel<T>, dim3(nb), dim3(kThreads), 0, st, n, w, static_cast<const T *>(V),
+                       j + 1, c, part, counter);
+    if (e == cudaSuccess)
+        e = launch_pdl(cgs_update_norm_kernel<T>, dim3(nb), dim3(kThreads), 0, st, n, w, static_cast<const T *>(V),
+                       j, c, stat, part, counter);
+    if (e == cudaSuccess && j + 1 < m)
+        e = launch_pdl(scale_next_kernel<T>, dim3(nb), dim3(kThreads), 0, st, n, static_cast<const T *>(w),
+                       V + (int64_t)(j + 1) * n, static_cast<const ArnoldiCtrl *>(c));
+    return e;
 }
 
 template <typename T>

@@ -103,19 +103,17 @@ cudaError_t Gmres<VT>::solve_device(const StopOp &A, const StopOp *P, const VT *
     res->launches += 3;
     int last_stop = 0;
     for (;;) {
-        // the start of a cycle may already stop the solve (zero or non-finite
-        // residual): learn that before queuing steps
-        RF_TRY(cudaStreamSynchronize(st_));
-        last_stop = hs[kArnoldiMax].stop;
-        if (last_stop == 3) {
-            res->info = kInfoNaN;
-            return cudaSuccess;
-        }
-        if (last_stop) {
-            res->info = 0;
-            return cudaSuccess;
-        }
+        // The start of a cycle may already stop the solve (zero or non-finite
+        // residual).  Its outcome is read after the first step's event: steps
+        // queued behind a stopped start return at once and leave their
+        // outcome slots untouched.
         bool ahead = false;  // a step was queued after the one that stopped
+        int queued = 0;
+        int start_stop = -1;  // the start's outcome, once known
+        auto read_start = [&] {
+            if (start_stop < 0) start_stop = hs[kArnoldiMax].stop;
+            return start_stop != 0;
+        };
         for (int j = 0; j < m; ++j) {
             const VT *in = V_ + (size_t)j * n_;
             if (P) {
@@ -129,9 +127,11 @@ cudaError_t Gmres<VT>::solve_device(const StopOp &A, const StopOp *P, const VT *
                                                     rb_.max_blocks, st_));
             res->launches += 4;
             RF_TRY(cudaEventRecord(step_ev_[j], st_));
+            ++queued;
             if (j > 0) {
                 // step j is queued: now wait for step j - 1 (the GPU is busy with j)
                 RF_TRY(cudaEventSynchronize(step_ev_[j - 1]));
+                if (read_start()) break;
                 last_stop = hs[j - 1].stop;
                 res->iterations = hs[j - 1].itn;
                 res->backward_error = hs[j - 1].bea;
@@ -141,12 +141,24 @@ cudaError_t Gmres<VT>::solve_device(const StopOp &A, const StopOp *P, const VT *
                 }
             }
         }
-        if (!ahead) {
+        if (start_stop <= 0 && !ahead) {
             RF_TRY(cudaEventSynchronize(step_ev_[m - 1]));
-            last_stop = hs[m - 1].stop;
-            res->iterations = hs[m - 1].itn;
-            res->backward_error = hs[m - 1].bea;
-        } else {
+            if (!read_start()) {
+                last_stop = hs[m - 1].stop;
+                res->iterations = hs[m - 1].itn;
+                res->backward_error = hs[m - 1].bea;
+            }
+        }
+        if (start_stop > 0) {
+            // every step of this cycle returned at once
+            for (int q = 0; q < queued; ++q) {
+                res->matvecs--;
+                if (on_skipped_product) on_skipped_product();
+            }
+            res->info = start_stop == 3 ? kInfoNaN : 0;
+            return cudaSuccess;
+        }
+        if (ahead) {
             res->matvecs--;  // the queued step's product returned at once
             if (on_skipped_product) on_skipped_product();
         }

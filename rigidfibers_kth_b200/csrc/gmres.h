@@ -49,9 +49,11 @@ class Gmres {
     // Inner solve of the refinement, controlled on the device (arnoldi.cu):
     // x = 0 initially, stop on the Arnoldi estimate <= tol or the budget,
     // CGS2 orthogonalisation.  The host queues each step before it learns
-    // whether the previous one stopped; a step queued after the stop runs as
-    // empty launches, and `on_skipped_product` is called once for its
-    // product (the caller's product timer drops it).  Needs m <= kArnoldiMax.
+    // whether the previous one stopped (the first steps of a cycle also
+    // before it learns whether the cycle's start stopped); a step queued
+    // after the stop runs as empty launches, and `on_skipped_product` is
+    // called once for each such product (the caller's product timer drops
+    // it).  Needs m <= kArnoldiMax.
     cudaError_t solve_device(const StopOp &A, const StopOp *P, const VT *b, VT *x, double tol, int max_iters,
                              GmresResult *res, const std::function<void()> &on_skipped_product);
     int restart() const { return m_; }

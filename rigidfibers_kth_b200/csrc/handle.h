@@ -41,6 +41,7 @@ struct rf_handle {
     double *lu_r = nullptr;    // direct solver: residual b - A x for the statistics
     int *lu_piv = nullptr;     // [n] pivot rows
     int *lu_info = nullptr;
+    void *blas = nullptr;      // direct solver: cuBLAS handle (cublasHandle_t), made at the first direct solve
     float *A32 = nullptr;
     __nv_bfloat16 *A16 = nullptr;   // BF16 matrix; in split storage also the high plane
     unsigned short *A16lo = nullptr;  // split storage (mixed BF16): the low plane, a_plane entries after A16

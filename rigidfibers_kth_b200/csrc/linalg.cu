@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(kGemvThreads, GemvMinBlocks<ACC>::value) gemv_
                                                                     int64_t cols_per_split, ACC *__restrict__ work,
                                                                     int64_t mpad, const int *__restrict__ stop,
                                                                     int64_t plane) {
+    pdl_wait();
     if (stop && *stop) return;  // a speculatively queued product of a finished solve
     constexpr int VEC = Vec16<S>::kVec;
     const int64_t row = ((int64_t)blockIdx.x * kGemvThreads + threadIdx.x) * VEC;
@@ -154,6 +155,7 @@ __global__ void __launch_bounds__(kGemvThreads, GemvMinBlocks<ACC>::value) gemv_
 template <typename ACC, typename Y>
 __global__ void gemv_reduce_kernel(const ACC *__restrict__ work, int splits, int64_t mpad, int64_t m, Y *y,
                                    const Y *r, const int *__restrict__ stop) {
+    pdl_wait();
     if (stop && *stop) return;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
@@ -226,11 +228,11 @@ cudaError_t launch_gemv(const S *A, int64_t lda, int64_t m, int64_t k, const X *
     if ((int64_t)splits * mpad > work_elems) return cudaErrorInvalidValue;
     const int64_t cps = (k + splits - 1) / splits;
     dim3 grid((unsigned)tiles, (unsigned)splits);
-    gemv_partial_kernel<S, X, ACC><<<grid, kGemvThreads, 0, st>>>(A, lda, m, k, x, cps, work, mpad, stop, plane);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_pdl(gemv_partial_kernel<S, X, ACC>, grid, dim3(kGemvThreads), 0, st, A, lda, m, k, x, cps,
+                               work, mpad, stop, plane);
     if (e != cudaSuccess) return e;
-    gemv_reduce_kernel<ACC, Y><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(work, splits, mpad, m, y, r, stop);
-    return cudaGetLastError();
+    return launch_pdl(gemv_reduce_kernel<ACC, Y>, dim3((unsigned)((m + 255) / 256)), dim3(256), 0, st,
+                      static_cast<const ACC *>(work), splits, mpad, m, y, r, stop);
 }
 
 template cudaError_t launch_gemv<double, double, double, double>(const double *, int64_t, int64_t, int64_t,
@@ -437,6 +439,7 @@ template <typename T>
 __global__ void __launch_bounds__(kApplyFibers * kApplyMaxNb) pair_apply_kernel(
     int M, int nb, int kp, int pstride, const float *__restrict__ B, const int *__restrict__ knn, int kstride,
     double omega, const T *__restrict__ v, T *__restrict__ z, const int *__restrict__ stop) {
+    pdl_wait();
     if (stop && *stop) return;
     __shared__ int s_j[kApplyFibers * kApplyMaxKp];
     __shared__ T s_v[kApplyFibers * kApplyMaxKp * kApplyMaxNb];
@@ -555,9 +558,8 @@ template <typename T>
 cudaError_t launch_pair_apply(int M, int nb, int kp, int pstride, const float *B, const int *knn, int kstride,
                               double omega, const T *v, T *z, cudaStream_t st, const int *stop) {
     if (nb > kApplyMaxNb || kp > kApplyMaxKp) return cudaErrorInvalidValue;
-    pair_apply_kernel<T><<<(unsigned)((M + kApplyFibers - 1) / kApplyFibers), kApplyFibers * nb, 0, st>>>(
-        M, nb, kp, pstride, B, knn, kstride, omega, v, z, stop);
-    return cudaGetLastError();
+    return launch_pdl(pair_apply_kernel<T>, dim3((unsigned)((M + kApplyFibers - 1) / kApplyFibers)),
+                      dim3(kApplyFibers * nb), 0, st, M, nb, kp, pstride, B, knn, kstride, omega, v, z, stop);
 }
 
 template cudaError_t launch_mgs_step<double>(int64_t, double *, const double *, const double *, const double *,

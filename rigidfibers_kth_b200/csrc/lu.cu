@@ -3,7 +3,7 @@
 //
 // Reference: LAPACK dgesv called by fortran/coeffs_and_vels.f90:62,158,333,514
 // (the *_direct golden runs).  Blocked right-looking factorisation, panel
-// width kLuNb:
+// width kLuNb = 64:
 //   lu_panel_kernel  one CTA factors 8 columns of the tall panel
 //                    A[k:n, k:k+nb]: per column the pivot (first row of
 //                    largest magnitude, as idamax), the row swap across the
@@ -14,11 +14,16 @@
 //                    over the whole GPU;
 //   lu_swap_kernel   the panel's row swaps applied to the trailing columns;
 //   lu_trsm_kernel   U12 = L11^-1 A12, one thread per trailing column;
-//   lu_gemm_kernel   A22 -= L21 U12, 64 x 64 tiles staged in shared memory.
+//   cublasDgemm      A22 -= L21 U12, the rank-64 trailing update (a plain
+//                    GEMM: most of the 2/3 n^3 flops).  The wider panel
+//                    halves the passes over the trailing matrix that
+//                    32-column panels needed.
 // The swaps are not applied to the L columns left of a panel: the forward
 // solve applies each panel's swaps to the right-hand side just before that
 // panel's columns of L, which is the same elimination (LINPACK's order).
 // Info as LAPACK: the first zero pivot (1-based), 0 when there is none.
+#include <cublas_v2.h>
+
 #include <algorithm>
 
 #include "rf_kernels.h"
@@ -26,7 +31,7 @@
 namespace rf {
 namespace {
 
-constexpr int kLuNb = 32;
+constexpr int kLuNb = 64;
 constexpr int kLuSub = 8;   // sub-panel width: the columns one CTA factors
 constexpr int kPanelThreads = 1024;
 
@@ -192,53 +197,8 @@ __global__ void __launch_bounds__(128) lu_trsm_kernel(double *A, int64_t lda, in
         if (i < nb) col[i] = x[i];
 }
 
-// A22 -= L21 U12 over rows and columns [k + nb, n): 64 x 64 tiles, 256 threads,
-// 4 x 4 entries per thread (rows tx + 16 i, columns ty + 16 j: consecutive
-// threads touch consecutive rows of a column).
-__global__ void __launch_bounds__(256) lu_gemm_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb) {
-    __shared__ double s_a[kLuNb][64];      // L21 tile: [p][row]
-    __shared__ double s_b[64][kLuNb + 1];  // U12 tile: [column][p]
-    const int64_t base = k + nb;
-    const int64_t r0 = base + blockIdx.x * 64, c0 = base + blockIdx.y * 64;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    for (int t = tid; t < kLuNb * 64; t += 256) {
-        const int p = t / 64, r = t % 64;
-        s_a[p][r] = (p < nb && r0 + r < n) ? A[(k + p) * lda + r0 + r] : 0.0;
-        const int cc = t / kLuNb, q = t % kLuNb;
-        s_b[cc][q] = (q < nb && c0 + cc < n) ? A[(c0 + cc) * lda + k + q] : 0.0;
-    }
-    __syncthreads();
-    double acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
-#pragma unroll 8
-    for (int p = 0; p < kLuNb; ++p) {
-        double a[4], b[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = s_a[p][tx + 16 * i];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = s_b[ty + 16 * j][p];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int64_t c = c0 + ty + 16 * j;
-        if (c >= n) continue;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int64_t r = r0 + tx + 16 * i;
-            if (r < n) A[c * lda + r] -= acc[i][j];
-        }
-    }
-}
-
 // Forward solve, panel k: the panel's swaps on x, then the unit lower
-// triangle L11 (one thread, nb <= 32 rows).
+// triangle L11 (one thread, nb <= kLuNb rows).
 __global__ void lu_fwd_diag_kernel(const double *A, int64_t lda, int64_t k, int nb, const int *piv, double *x) {
     for (int j = 0; j < nb; ++j) {
         const int64_t p = piv[k + j];
@@ -278,7 +238,12 @@ int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 }  // namespace
 
-cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, cudaStream_t st, int64_t *launches) {
+cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, void *blas, cudaStream_t st,
+                      int64_t *launches) {
+    if (!blas || lda > INT32_MAX || n > INT32_MAX) return cudaErrorInvalidValue;
+    cublasHandle_t bh = static_cast<cublasHandle_t>(blas);
+    if (cublasSetStream(bh, st) != CUBLAS_STATUS_SUCCESS) return cudaErrorUnknown;
+    const double minus_one = -1.0, one = 1.0;
     cudaError_t e = cudaMemsetAsync(info, 0, sizeof(int), st);
     for (int64_t k = 0; k < n && e == cudaSuccess; k += kLuNb) {
         const int nb = (int)std::min<int64_t>(kLuNb, n - k);
@@ -296,10 +261,15 @@ cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, cu
         if (rest > 0) {
             lu_swap_kernel<<<(unsigned)cdiv(rest, 128), 128, 0, st>>>(A, lda, n, k, nb, k + nb, piv);
             lu_trsm_kernel<<<(unsigned)cdiv(rest, 128), 128, 0, st>>>(A, lda, n, k, nb);
-            lu_gemm_kernel<<<dim3((unsigned)cdiv(rest, 64), (unsigned)cdiv(rest, 64)), 256, 0, st>>>(A, lda, n, k, nb);
-            *launches += 3;
+            *launches += 2;  // the GEMM below is cuBLAS's
+            e = cudaGetLastError();
+            if (e != cudaSuccess) break;
+            const int r = (int)rest, ld = (int)lda;
+            if (cublasDgemm(bh, CUBLAS_OP_N, CUBLAS_OP_N, r, r, nb, &minus_one, A + k * lda + k + nb, ld,
+                            A + (k + nb) * lda + k, ld, &one, A + (k + nb) * lda + k + nb, ld) != CUBLAS_STATUS_SUCCESS)
+                return cudaErrorUnknown;
         }
-        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaGetLastError();
     }
     return e;
 }

@@ -47,6 +47,28 @@ __device__ __forceinline__ double load_entry<SplitF32>(const SplitF32 *A, int64_
     return (double)__uint_as_float(split_join(hi, lo));
 }
 
+// Programmatic dependent launch: a kernel launched by launch_pdl may be
+// scheduled while the previous kernel on the stream finishes; it must call
+// pdl_wait() before its first global memory access, which returns once that
+// kernel has completed and its writes are visible.  Saves the launch gap of
+// the short kernels of an inner GMRES step.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 struct AsmArgs {
     int M, N, LQ;
     int t0, t1;                // target fibers [t0, t1) (a row-block shard; 0, M for the whole system)
@@ -96,10 +118,12 @@ struct SplitArgs {
     double near_c;             // c below which a pair is near
 };
 constexpr int kNearBlockFloats = 320;
-// Smallest near threshold of the split assembly: from c = 6 on, the FP32
-// backward recursion run from n = 32 down to n = 0 (moments_backward_fp32) is
-// accurate to FP32 rounding in every direction, on the source axis included.
-constexpr double kSplitMinNearC = 6.0;
+// Smallest near threshold of the split assembly: from c = 5 on, the FP32
+// backward recursion run from n = 32 down to n = 0 (moments_backward_fp32)
+// keeps the Legendre combinations within 1e-6 of |X_0| in every direction,
+// on the source axis included (at c = 4 the error of the truncated start
+// reaches 5e-6).
+constexpr double kSplitMinNearC = 5.0;
 bool split_supported(int N, int LQ);
 int split_far_chunks(int M, int sm_count);
 cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st);
@@ -184,8 +208,10 @@ cudaError_t launch_dot(int64_t n, const T *a, const T *b, double *out, const Red
 // Direct solve (lu.cu): A (n x n, column-major, ld lda) is overwritten by its
 // LU factors with partial pivoting, piv[n] the pivot rows (0-based), info the
 // first zero pivot (1-based) or 0; lu_solve overwrites x (= b on entry) with
-// the solution.  launches counts the kernels launched.
-cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, cudaStream_t st, int64_t *launches);
+// the solution.  blas: a cuBLAS handle (the trailing updates); launches counts
+// the kernels launched.
+cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, void *blas, cudaStream_t st,
+                      int64_t *launches);
 cudaError_t lu_solve(const double *A, int64_t lda, int64_t n, const int *piv, double *x, cudaStream_t st,
                      int64_t *launches);
 // y = alpha_scale * x where alpha_scale = num/den (den device scalar), i.e. y = x * (num / *den)
