@@ -33,7 +33,8 @@ namespace {
 
 constexpr int kLuNb = 64;
 constexpr int kLuSub = 8;   // sub-panel width: the columns one CTA factors
-constexpr int kPanelThreads = 1024;
+constexpr int kPanelThreads = 512;
+constexpr int kRowBatch = 4;  // rows per thread whose loads are issued together in the panel's passes
 
 __device__ __forceinline__ void argmax_merge(double &v, int64_t &i, double ov, int64_t oi) {
     if (ov > v || (ov == v && oi < i)) {
@@ -104,14 +105,35 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int6
         const double inv = d != 0.0 ? 1.0 / d : 0.0;  // a zero pivot leaves a zero column (dgetf2)
         best = -1.0;
         bi = n;
-        for (int64_t r = col + 1 + tid; r < n; r += blockDim.x) {
-            const double x = d != 0.0 ? cj[r] * inv : cj[r];
-            cj[r] = x;
-            for (int c = j + 1; c < sb; ++c) {
-                double *cc = A + (s0 + c) * lda;
-                const double v = fma(-x, s_u[c], cc[r]);
-                cc[r] = v;
-                if (c == j + 1) argmax_merge(best, bi, fabs(v), r);
+        // kRowBatch rows per thread and round: all their loads are issued
+        // before the stores (the stores of one row could otherwise hold back
+        // the loads of the next); the pivot search is order-independent
+        for (int64_t rb = col + 1 + tid; rb < n; rb += (int64_t)kRowBatch * blockDim.x) {
+            double xs[kRowBatch], vs[kRowBatch][kLuSub];
+#pragma unroll
+            for (int u = 0; u < kRowBatch; ++u) {
+                const int64_t r = rb + (int64_t)u * blockDim.x;
+                if (r < n) {
+                    xs[u] = cj[r];
+#pragma unroll
+                    for (int c = 0; c < kLuSub; ++c)
+                        if (c > j && c < sb) vs[u][c] = A[(s0 + c) * lda + r];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRowBatch; ++u) {
+                const int64_t r = rb + (int64_t)u * blockDim.x;
+                if (r < n) {
+                    const double x = d != 0.0 ? xs[u] * inv : xs[u];
+                    cj[r] = x;
+#pragma unroll
+                    for (int c = 0; c < kLuSub; ++c)
+                        if (c > j && c < sb) {
+                            const double v = fma(-x, s_u[c], vs[u][c]);
+                            A[(s0 + c) * lda + r] = v;
+                            if (c == j + 1) argmax_merge(best, bi, fabs(v), r);
+                        }
+                }
             }
         }
         if (j + 1 < sb) p = block_argmax(best, bi, n, s_val, s_idx);
@@ -198,30 +220,77 @@ __global__ void __launch_bounds__(128) lu_trsm_kernel(double *A, int64_t lda, in
 }
 
 // Forward solve, panel k: the panel's swaps on x, then the unit lower
-// triangle L11 (one thread, nb <= kLuNb rows).
-__global__ void lu_fwd_diag_kernel(const double *A, int64_t lda, int64_t k, int nb, const int *piv, double *x) {
-    for (int j = 0; j < nb; ++j) {
-        const int64_t p = piv[k + j];
-        if (p != k + j) {
-            const double t = x[k + j];
-            x[k + j] = x[p];
-            x[p] = t;
+// triangle L11; one CTA of kLuNb threads.  The rows the swaps touch (the
+// panel's nb rows and up to nb pivot rows below) are loaded at once, the
+// swaps applied in order in shared memory and the rows written back; then
+// L11 from shared memory, one column per step.
+__global__ void __launch_bounds__(kLuNb) lu_fwd_diag_kernel(const double *A, int64_t lda, int64_t k, int nb,
+                                                            const int *piv, double *x) {
+    __shared__ double s_l[kLuNb][kLuNb + 1];
+    __shared__ double s_x[2 * kLuNb];
+    __shared__ int64_t s_p[kLuNb];
+    __shared__ int s_slot[kLuNb];
+    const int t = threadIdx.x;
+    if (t < nb) {
+        s_p[t] = piv[k + t];
+        s_x[t] = x[k + t];
+        for (int p = 0; p < nb; ++p) s_l[t][p] = A[(k + p) * lda + k + t];
+    }
+    __syncthreads();
+    if (t < nb) {
+        // slot of pivot row p_t: inside the panel its own row, below it the
+        // slot of the first swap that names the same row
+        const int64_t p = s_p[t];
+        int slot = (int)(p - k);
+        if (p >= k + nb) {
+            slot = kLuNb + t;
+            for (int q = 0; q < t; ++q)
+                if (s_p[q] == p) {
+                    slot = kLuNb + q;
+                    break;
+                }
+            if (slot == kLuNb + t) s_x[slot] = x[p];
         }
+        s_slot[t] = slot;
     }
-    for (int i = 1; i < nb; ++i) {
-        double s = x[k + i];
-        for (int p = 0; p < i; ++p) s = fma(-A[(k + p) * lda + k + i], x[k + p], s);
-        x[k + i] = s;
+    __syncthreads();
+    if (t == 0)
+        for (int q = 0; q < nb; ++q) {
+            const int o = s_slot[q];
+            if (o != q) {
+                const double v = s_x[q];
+                s_x[q] = s_x[o];
+                s_x[o] = v;
+            }
+        }
+    __syncthreads();
+    if (t < nb && s_slot[t] == kLuNb + t) x[s_p[t]] = s_x[kLuNb + t];
+    for (int p = 0; p + 1 < nb; ++p) {
+        if (t > p && t < nb) s_x[t] = fma(-s_l[t][p], s_x[p], s_x[t]);
+        __syncthreads();
     }
+    if (t < nb) x[k + t] = s_x[t];
 }
 
-// Backward solve, panel k: the upper triangle U11 (one thread).
-__global__ void lu_bwd_diag_kernel(const double *A, int64_t lda, int64_t k, int nb, double *x) {
-    for (int i = nb - 1; i >= 0; --i) {
-        double s = x[k + i];
-        for (int p = i + 1; p < nb; ++p) s = fma(-A[(k + p) * lda + k + i], x[k + p], s);
-        x[k + i] = s / A[(k + i) * lda + k + i];
+// Backward solve, panel k: the upper triangle U11, one CTA of kLuNb threads,
+// U11 from shared memory, one column per step (last first).
+__global__ void __launch_bounds__(kLuNb) lu_bwd_diag_kernel(const double *A, int64_t lda, int64_t k, int nb,
+                                                            double *x) {
+    __shared__ double s_u[kLuNb][kLuNb + 1];
+    __shared__ double s_x[kLuNb];
+    const int t = threadIdx.x;
+    if (t < nb) {
+        s_x[t] = x[k + t];
+        for (int p = 0; p < nb; ++p) s_u[t][p] = A[(k + p) * lda + k + t];
     }
+    __syncthreads();
+    for (int p = nb - 1; p >= 0; --p) {
+        if (t == p) s_x[p] = s_x[p] / s_u[p][p];
+        __syncthreads();
+        if (t < p) s_x[t] = fma(-s_u[t][p], s_x[p], s_x[t]);
+        __syncthreads();
+    }
+    if (t < nb) x[k + t] = s_x[t];
 }
 
 // x[r] -= sum_p A[r, k + p] x[k + p] for rows r in [r0, r1): the panel's
@@ -279,7 +348,7 @@ cudaError_t lu_solve(const double *A, int64_t lda, int64_t n, const int *piv, do
     cudaError_t e = cudaSuccess;
     for (int64_t k = 0; k < n && e == cudaSuccess; k += kLuNb) {
         const int nb = (int)std::min<int64_t>(kLuNb, n - k);
-        lu_fwd_diag_kernel<<<1, 1, 0, st>>>(A, lda, k, nb, piv, x);
+        lu_fwd_diag_kernel<<<1, kLuNb, 0, st>>>(A, lda, k, nb, piv, x);
         ++*launches;
         if (k + nb < n) {
             lu_update_kernel<<<(unsigned)cdiv(n - k - nb, 256), 256, 0, st>>>(A, lda, k, nb, k + nb, n, x);
@@ -290,7 +359,7 @@ cudaError_t lu_solve(const double *A, int64_t lda, int64_t n, const int *piv, do
     const int64_t last = ((n - 1) / kLuNb) * kLuNb;
     for (int64_t k = last; k >= 0 && e == cudaSuccess; k -= kLuNb) {
         const int nb = (int)std::min<int64_t>(kLuNb, n - k);
-        lu_bwd_diag_kernel<<<1, 1, 0, st>>>(A, lda, k, nb, x);
+        lu_bwd_diag_kernel<<<1, kLuNb, 0, st>>>(A, lda, k, nb, x);
         ++*launches;
         if (k > 0) {
             lu_update_kernel<<<(unsigned)cdiv(k, 256), 256, 0, st>>>(A, lda, k, nb, 0, k, x);
