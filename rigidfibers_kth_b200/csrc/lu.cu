@@ -4,8 +4,8 @@
 // Reference: LAPACK dgesv called by fortran/coeffs_and_vels.f90:62,158,333,514
 // (the *_direct golden runs).  Blocked right-looking factorisation, panel
 // width kLuNb = 64:
-//   lu_panel_kernel  one CTA factors 8 columns of the tall panel
-//                    A[k:n, k:k+nb]: per column the pivot (first row of
+//   lu_panel_kernel  a cluster of 8 CTAs factors 8 columns of the tall
+//                    panel A[k:n, k:k+nb]: per column the pivot (first row of
 //                    largest magnitude, as idamax), the row swap across the
 //                    panel, the scaling by the reciprocal pivot and the rank-1
 //                    update of the 8 columns (dgetf2's steps; the last three
@@ -22,6 +22,7 @@
 // solve applies each panel's swaps to the right-hand side just before that
 // panel's columns of L, which is the same elimination (LINPACK's order).
 // Info as LAPACK: the first zero pivot (1-based), 0 when there is none.
+#include <cooperative_groups.h>
 #include <cublas_v2.h>
 
 #include <algorithm>
@@ -31,10 +32,13 @@
 namespace rf {
 namespace {
 
+namespace cg = cooperative_groups;
+
 constexpr int kLuNb = 64;
 constexpr int kLuSub = 8;   // sub-panel width: the columns one CTA factors
 constexpr int kPanelThreads = 512;
-constexpr int kRowBatch = 4;  // rows per thread whose loads are issued together in the panel's passes
+constexpr int kRowBatch = 2;  // rows per thread whose loads are issued together in the panel's passes
+constexpr int kPanelCluster = 8;  // CTAs (SMs) that factor one sub-panel together
 
 __device__ __forceinline__ void argmax_merge(double &v, int64_t &i, double ov, int64_t oi) {
     if (ov > v || (ov == v && oi < i)) {
@@ -44,9 +48,9 @@ __device__ __forceinline__ void argmax_merge(double &v, int64_t &i, double ov, i
 }
 
 // Block-wide first-maximum reduction of (value, row) pairs; every thread gets
-// the result.
+// the row (and, in *vmax, the value).
 __device__ __forceinline__ int64_t block_argmax(double best, int64_t bi, int64_t none, double *s_val,
-                                                int64_t *s_idx) {
+                                                int64_t *s_idx, double *vmax) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     for (int o = 16; o; o >>= 1)
         argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, o), __shfl_down_sync(0xffffffffu, bi, o));
@@ -60,47 +64,83 @@ __device__ __forceinline__ int64_t block_argmax(double best, int64_t bi, int64_t
         bi = lane < nwarps ? s_idx[lane] : none;
         for (int o = 16; o; o >>= 1)
             argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, o), __shfl_down_sync(0xffffffffu, bi, o));
-        if (lane == 0) s_idx[0] = bi;
+        if (lane == 0) {
+            s_idx[0] = bi;
+            s_val[0] = best;
+        }
     }
     __syncthreads();
     const int64_t r = s_idx[0];
+    *vmax = s_val[0];
     __syncthreads();  // s_idx is reused by the next reduction
     return r;
 }
 
 // Sub-panel factorisation: columns [s0, s0 + sb) of the panel [k, k + nb),
-// one CTA.  One pass per column over the rows below the diagonal: scale the
-// column by the reciprocal pivot, update the sub-panel's remaining columns
-// (the pivot row's entries staged in shared memory) and, in the same pass,
-// find the next column's pivot among the updated values.  Row swaps cover
-// all nb columns of the panel, so its L is consistent.  Then U of the
-// sub-panel's rows for the panel's columns right of it (unit lower sb x sb
-// triangle, one thread per column).
-__global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb,
-                                                                int64_t s0, int sb, int *piv, int *info) {
+// on one cluster of kPanelCluster CTAs (one per SM), the rows below the
+// diagonal interleaved over all their threads.  One pass per column over
+// those rows: scale the column by the reciprocal pivot, update the
+// sub-panel's remaining columns (the pivot row's entries staged in shared
+// memory) and, in the same pass, find the next column's pivot among the
+// updated values.  Each CTA's candidate (value, row) goes to a slot in the
+// shared memory of the cluster's first CTA, and every CTA merges the slots
+// in the same way (first maximum: the same pivot as one CTA over all rows).
+// Row swaps (by the first CTA) cover all nb columns of the panel, so its L
+// is consistent.  Then U of the sub-panel's rows for the panel's columns
+// right of it (unit lower sb x sb triangle, one thread per column).
+// Every thread of the cluster passes the same 1 + 2 sb cluster barriers.
+__global__ void __cluster_dims__(kPanelCluster, 1, 1) __launch_bounds__(kPanelThreads)
+    lu_panel_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb, int64_t s0, int sb, int *piv, int *info) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned rank = cluster.block_rank();
     __shared__ double s_val[kPanelThreads / 32];
     __shared__ int64_t s_idx[kPanelThreads / 32];
     __shared__ double s_u[kLuSub];
+    __shared__ double c_val[kPanelCluster];   // pivot candidates (the first CTA's copy is used)
+    __shared__ int64_t c_idx[kPanelCluster];
+    double *r_val = cluster.map_shared_rank(c_val, 0);
+    int64_t *r_idx = cluster.map_shared_rank(c_idx, 0);
     const int tid = threadIdx.x;
+    const int64_t g = (int64_t)rank * kPanelThreads + tid;  // this thread's offset among the cluster's rows
+    constexpr int64_t kStride = (int64_t)kPanelCluster * kPanelThreads;
+    // the cluster's first maximum; ends with the row pass's stores visible
+    // to every CTA (fence, then the barrier)
+    auto cluster_argmax = [&](double best, int64_t bi) -> int64_t {
+        double v;
+        const int64_t r = block_argmax(best, bi, n, s_val, s_idx, &v);
+        if (tid == 0) {
+            r_val[rank] = v;
+            r_idx[rank] = r;
+        }
+        __threadfence();
+        cluster.sync();
+        double bv = -1.0;
+        int64_t bidx = n;
+        for (int q = 0; q < kPanelCluster; ++q) argmax_merge(bv, bidx, r_val[q], r_idx[q]);
+        return bidx;
+    };
     double best = -1.0;
     int64_t bi = n;
-    for (int64_t r = s0 + tid; r < n; r += blockDim.x) argmax_merge(best, bi, fabs(A[s0 * lda + r]), r);
-    int64_t p = block_argmax(best, bi, n, s_val, s_idx);
+    for (int64_t r = s0 + g; r < n; r += kStride) argmax_merge(best, bi, fabs(A[s0 * lda + r]), r);
+    int64_t p = cluster_argmax(best, bi);
     for (int j = 0; j < sb; ++j) {
         const int64_t col = s0 + j;
         if (p >= n) p = col;  // a column of NaN keeps its row
-        if (tid == 0) piv[col] = (int)p;
-        if (p != col && tid < nb) {
-            double *c = A + (k + tid) * lda;
-            const double t = c[col];
-            c[col] = c[p];
-            c[p] = t;
+        if (rank == 0) {
+            if (tid == 0) piv[col] = (int)p;
+            if (p != col && tid < nb) {
+                double *c = A + (k + tid) * lda;
+                const double t = c[col];
+                c[col] = c[p];
+                c[p] = t;
+            }
         }
-        __syncthreads();
+        __threadfence();
+        cluster.sync();  // the swapped rows, seen by every CTA
         double *cj = A + col * lda;
         const double d = cj[col];
         if (tid < sb) s_u[tid] = tid > j ? A[(s0 + tid) * lda + col] : 0.0;
-        if (d == 0.0 && tid == 0 && *info == 0) *info = (int)(col + 1);
+        if (rank == 0 && d == 0.0 && tid == 0 && *info == 0) *info = (int)(col + 1);
         __syncthreads();
         const double inv = d != 0.0 ? 1.0 / d : 0.0;  // a zero pivot leaves a zero column (dgetf2)
         best = -1.0;
@@ -108,11 +148,11 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int6
         // kRowBatch rows per thread and round: all their loads are issued
         // before the stores (the stores of one row could otherwise hold back
         // the loads of the next); the pivot search is order-independent
-        for (int64_t rb = col + 1 + tid; rb < n; rb += (int64_t)kRowBatch * blockDim.x) {
+        for (int64_t rb = col + 1 + g; rb < n; rb += (int64_t)kRowBatch * kStride) {
             double xs[kRowBatch], vs[kRowBatch][kLuSub];
 #pragma unroll
             for (int u = 0; u < kRowBatch; ++u) {
-                const int64_t r = rb + (int64_t)u * blockDim.x;
+                const int64_t r = rb + (int64_t)u * kStride;
                 if (r < n) {
                     xs[u] = cj[r];
 #pragma unroll
@@ -122,7 +162,7 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int6
             }
 #pragma unroll
             for (int u = 0; u < kRowBatch; ++u) {
-                const int64_t r = rb + (int64_t)u * blockDim.x;
+                const int64_t r = rb + (int64_t)u * kStride;
                 if (r < n) {
                     const double x = d != 0.0 ? xs[u] * inv : xs[u];
                     cj[r] = x;
@@ -136,12 +176,16 @@ __global__ void __launch_bounds__(kPanelThreads) lu_panel_kernel(double *A, int6
                 }
             }
         }
-        if (j + 1 < sb) p = block_argmax(best, bi, n, s_val, s_idx);
-        else __syncthreads();
+        if (j + 1 < sb) {
+            p = cluster_argmax(best, bi);
+        } else {
+            __threadfence();
+            cluster.sync();  // every CTA's rows written before the U rows below read them
+        }
     }
     // U rows of the sub-panel for the panel's columns right of it
     const int64_t c = s0 + sb + tid;
-    if (c < k + nb && c < n) {
+    if (rank == 0 && c < k + nb && c < n) {
         double *col = A + c * lda + s0;
         for (int i = 1; i < sb; ++i) {
             double v = col[i];
@@ -318,7 +362,7 @@ cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, vo
         const int nb = (int)std::min<int64_t>(kLuNb, n - k);
         for (int s0 = 0; s0 < nb; s0 += kLuSub) {
             const int sb = std::min(kLuSub, nb - s0);
-            lu_panel_kernel<<<1, kPanelThreads, 0, st>>>(A, lda, n, k, nb, k + s0, sb, piv, info);
+            lu_panel_kernel<<<kPanelCluster, kPanelThreads, 0, st>>>(A, lda, n, k, nb, k + s0, sb, piv, info);
             ++*launches;
             if (s0 + sb < nb && k + s0 + sb < n) {
                 lu_panel_update_kernel<<<(unsigned)cdiv(n - k - s0 - sb, 256), 256, 0, st>>>(A, lda, n, k, nb, k + s0,

@@ -79,7 +79,7 @@ def test_two_steps_match_golden(golden, case):
 
 @pytest.mark.parametrize("M", [100, 300])
 def test_direct_solver_matches_oracle_lu(M):
-    """Device LU with partial pivoting (panels of 32; n = 1500 and 4500, the
+    """Device LU with partial pivoting (panels of 64; n = 1500 and 4500, the
     last panel partial) against the oracle's LU (LAPACK dgesv's algorithm) of
     the same matrix: coefficients within 1e-10, the device's backward error at
     rounding level, and A left in place (the factors have their own buffer)."""
