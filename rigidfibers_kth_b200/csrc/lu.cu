@@ -197,11 +197,15 @@ __global__ void __cluster_dims__(kPanelCluster, 1, 1) __launch_bounds__(kPanelTh
 
 // The sub-panel's rank-sb update of the panel's columns right of it:
 // A[r, c] -= sum_q A[r, s0 + q] A[s0 + q, c] for rows r >= s0 + sb and columns
-// c in [s0 + sb, k + nb); one thread per row, the U entries in shared memory.
-__global__ void __launch_bounds__(256) lu_panel_update_kernel(double *A, int64_t lda, int64_t n, int64_t k, int nb,
-                                                             int64_t s0, int sb) {
-    __shared__ double s_uu[kLuNb][kLuSub];
-    const int64_t c0 = s0 + sb, c1 = std::min<int64_t>(k + nb, n);
+// c in [s0 + sb, k + nb); one thread per row and group of kUpdCols columns
+// (blockIdx.y), the U entries in shared memory.
+constexpr int kUpdCols = 8;
+constexpr int kUpdThreads = 128;
+__global__ void __launch_bounds__(kUpdThreads) lu_panel_update_kernel(double *A, int64_t lda, int64_t n, int64_t k,
+                                                                      int nb, int64_t s0, int sb) {
+    __shared__ double s_uu[kUpdCols][kLuSub];
+    const int64_t c0 = s0 + sb + (int64_t)blockIdx.y * kUpdCols;
+    const int64_t c1 = std::min<int64_t>(std::min<int64_t>(k + nb, n), c0 + kUpdCols);
     const int nc = (int)(c1 - c0);
     for (int t = threadIdx.x; t < nc * sb; t += blockDim.x) {
         const int c = t / sb, q = t % sb;
@@ -365,8 +369,9 @@ cudaError_t lu_factor(double *A, int64_t lda, int64_t n, int *piv, int *info, vo
             lu_panel_kernel<<<kPanelCluster, kPanelThreads, 0, st>>>(A, lda, n, k, nb, k + s0, sb, piv, info);
             ++*launches;
             if (s0 + sb < nb && k + s0 + sb < n) {
-                lu_panel_update_kernel<<<(unsigned)cdiv(n - k - s0 - sb, 256), 256, 0, st>>>(A, lda, n, k, nb, k + s0,
-                                                                                          sb);
+                const dim3 grid((unsigned)cdiv(n - k - s0 - sb, kUpdThreads),
+                                (unsigned)cdiv(std::min<int64_t>(nb, n - k) - s0 - sb, kUpdCols));
+                lu_panel_update_kernel<<<grid, kUpdThreads, 0, st>>>(A, lda, n, k, nb, k + s0, sb);
                 ++*launches;
             }
         }
