@@ -120,10 +120,9 @@ typedef struct rf_params {
                                             fewest that reach gmres_tol with inner solves no deeper than
                                             this, each asking for an equal share of what is still needed */
     double near_field_c;                 /* mixed precision: squared distance below which the analytic
-                                            integral stays FP64 (default 5, also the smallest value
-                                            taken: from there on the FP32 backward recursion keeps the
-                                            moments within 1e-6 of their size; raised to 10 where the
-                                            tile kernel runs: numeric integration, N > 5);
+                                            integral stays FP64 (default 6: from there on the FP32
+                                            backward recursion reaches FP32 accuracy; raised to 10
+                                            where the tile kernel runs: numeric integration, N > 5);
                                             >= 1e30 keeps every integral in FP64 */
     int32_t shard_index;                 /* row-block shard of this handle (0 .. shard_count - 1) */
     int32_t shard_count;                 /* row-block shards (GPUs) the system is split over; 0 or 1: the

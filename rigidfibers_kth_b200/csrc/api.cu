@@ -258,7 +258,7 @@ void rf_params_default(rf_params *p) {
     p->max_refinements = 30;
     p->cluster_size = 8;
     p->inner_tol = 1e-3;
-    p->near_field_c = 5.0;
+    p->near_field_c = 6.0;
     p->pc_damping = kPcDamping;
 }
 

@@ -7,7 +7,7 @@
 // 16-bit planes of split storage (BF16 path; the high plane is the BF16
 // matrix of the inner solves).  A fiber pair (i, j) is "near"
 // when one of target i's quadrature points lies within sqrt(near_c) of source
-// j's centre (default c < 5: closer, the FP32 backward recursion loses digits;
+// j's centre (default c < 6: closer, the FP32 backward recursion loses digits;
 // the reference itself switches to forward recursion below 10).  Near pairs
 // are integrated in FP64, far pairs in FP32, every moment of a far pair by the
 // backward recursion run down to n = 0 (moments_backward_fp32: none of the
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
         };
         if (act) {
             if constexpr (FAR) {
-                // every point far (c >= near_c >= 5): two Gauss points per pass of the
+                // every point far (c >= 6): two Gauss points per pass of the
                 // packed recursion, added in the order q, q + 1.  Past an odd LQ
                 // the partner is the zero padding of s_pv: computed, not added.
                 static_assert(kMaxLQ % 2 == 0, "the partner of the last point must lie in s_pv");

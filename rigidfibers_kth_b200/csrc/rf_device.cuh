@@ -137,11 +137,10 @@ __device__ __forceinline__ void moments_fp64(double b, double c, double *I, doub
 // reaches n = 0 damped by c^(-n/2) (the recursion's homogeneous solutions grow
 // like |lambda|^n, lambda^2 + b lambda + c = 0, |lambda| = sqrt(c) since
 // d >= 0) times a polynomial in n that is largest for the S moments of a point
-// on the source axis.  From n = 32 that error is at FP32 rounding for every
-// c >= 5 and every direction: with sampled b, the Legendre combinations of the
-// moments stay within 9.1e-7 of |X_0| (X = I, J, S) at c = 5 (7.4e-7 at
-// c = 6) on and off the axis, 4.6e-6 at c = 4; from the reference's n = 27 the
-// on-axis S error is 1e-5 at c = 6.
+// on the source axis.  From n = 32 that error is below FP32 rounding for every
+// c >= 6 and every direction: with sampled b, the Legendre combinations of the
+// moments stay within 8e-7 of |X_0| (X = I, J, S) at c = 6, 6.5, 7, 8 on and
+// off the axis; from the reference's n = 27 the on-axis S error is 1e-5 at c = 6.
 constexpr int kBackTop = 32;
 
 // FP32 moments by the backward recursion alone, run down to n = 0.  The
@@ -154,7 +153,7 @@ constexpr int kBackTop = 32;
 // 100 fiber half-lengths apart loses every FP32 digit in them, and at a point
 // near the source axis the 1/d forms cancel too.  The recursion has neither
 // cancellation: ue - ub enters only as 2b / (ue + ub), and d not at all.
-// Accurate for c >= 5 in every direction (see kBackTop).
+// Accurate for c >= 6 in every direction (see kBackTop).
 template <int N>
 __device__ __forceinline__ void moments_backward_fp32(float b, float c, float *I, float *J, float *S) {
     constexpr int K = N + 3;
@@ -259,7 +258,7 @@ struct Geom32 {
 // forms rewritten without the cancellation te/ue - tb/ub (which loses all FP32
 // digits when the target point lies near the source axis):
 // te/ue - tb/ub = 2b d / ((te ub + tb ue) ue ub) when te and tb share a sign.
-// FAR = true: the caller guarantees c >= 5 (far pairs of the split assembly).
+// FAR = true: the caller guarantees c >= 6 (far pairs of the split assembly).
 template <int N, bool FAR = false>
 __device__ __forceinline__ void moments_fp32(const Geom32 &g, float *I, float *J, float *S) {
     const float b = g.b, c = g.c;

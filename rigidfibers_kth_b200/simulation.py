@@ -44,7 +44,7 @@ class FiberParams:
     max_refinements: int = 30
     cluster_size: int = 8
     inner_tol: float = 1e-3
-    near_field_c: float = 5.0
+    near_field_c: float = 6.0
     shard_index: int = 0
     shard_count: int = 1
     pc_damping: float = 0.85
