@@ -118,12 +118,12 @@ struct SplitArgs {
     double near_c;             // c below which a pair is near
 };
 constexpr int kNearBlockFloats = 320;
-// Smallest near threshold of the split assembly: from c = 5 on, the FP32
-// backward recursion run from n = 32 down to n = 0 (moments_backward_fp32)
-// keeps the Legendre combinations within 1e-6 of |X_0| in every direction,
-// on the source axis included (at c = 4 the error of the truncated start
-// reaches 5e-6).
-constexpr double kSplitMinNearC = 5.0;
+// Smallest near threshold of the split assembly: from c = 6 on, the FP32
+// backward recursion run from n = 32 down to n = 0 (moments_backward_fp32) is
+// accurate to FP32 rounding in every direction, on the source axis included.
+// (At c = 5 the truncated start already adds errors that lifted a velocity
+// error of an M = 8000 trajectory above 1e-6.)
+constexpr double kSplitMinNearC = 6.0;
 bool split_supported(int N, int LQ);
 int split_far_chunks(int M, int sm_count);
 cudaError_t launch_split_classify(const SplitArgs &a, cudaStream_t st);
