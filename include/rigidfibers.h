@@ -241,6 +241,18 @@ rf_status rf_get_solve_stats(rf_handle *h, rf_solve_stats *s);
  * the one array: calls that overlap on the GPU (other streams, other threads)
  * race on it.  Nothing in the array needs to start at zero. */
 rf_status rf_matvec_noalloc(const double *A, int64_t lda, int64_t n, const double *x, double *y, void *stream);
+/* Dense direct solve of a general system on the device, the LAPACK dgesv
+ * call of the reference's direct variant (fortran/coeffs_and_vels.f90:62,158,
+ * 333,514: dgesv(n, 1, A, n, ipiv, b, n, info)) without a handle, with the
+ * same device LU as use_direct_solver (partial pivoting, first row of largest
+ * magnitude).  A: host, n x n column-major with leading dimension lda >= n,
+ * left unchanged (the factors stay on the device); x = A^-1 b (host, n; may
+ * alias b); ipiv (host, n, or NULL): the pivot rows, 1-based as LAPACK's;
+ * *info: 0, or the first zero pivot (1-based; x is then undefined).  Runs on
+ * `device`, allocates one n x n FP64 copy of A there and returns when x is
+ * on the host; errors are read back with rf_last_error(NULL). */
+rf_status rf_dgesv(int64_t n, const double *A, int64_t lda, const double *b, double *x, int32_t *ipiv,
+                   int32_t *info, int32_t device);
 /* Multistep history for checkpoint/resume: previous positions/orientations
  * and previous velocities (3*M doubles each). */
 rf_status rf_get_history(rf_handle *h, double *prev_pos, double *prev_orient, double *prev_vel,

@@ -136,6 +136,8 @@ def lib():
         "rf_get_solve_stats": (ctypes.c_int, [_h, ctypes.POINTER(RfSolveStats)]),
         "rf_matvec_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_void_p]),
+        "rf_dgesv": (ctypes.c_int, [ctypes.c_int64, _dp, ctypes.c_int64, _dp, _dp, ctypes.c_void_p,
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]),
         "rf_get_history": (ctypes.c_int, [_h, _dp, _dp, _dp, _dp]),
         "rf_set_history": (ctypes.c_int, [_h, _dp, _dp, _dp, _dp, _dp]),
         "rf_timer_mark": (ctypes.c_int, [_h, ctypes.c_int32]),

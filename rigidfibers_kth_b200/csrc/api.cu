@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "handle.h"
 
@@ -1225,6 +1226,77 @@ rf_status rf_matvec(rf_handle *h, const double *x, double *y) {
     cudaFree(dx);
     cudaFree(dy);
     CK(h, e, "matvec");
+    return RF_OK;
+}
+
+rf_status rf_dgesv(int64_t n, const double *A, int64_t lda, const double *b, double *x, int32_t *ipiv,
+                   int32_t *info, int32_t device) {
+    if (!A || !b || !x || !info) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "rf_dgesv: null pointer");
+    if (n < 1 || lda < n || n > INT32_MAX) return rf::fail(nullptr, RF_ERR_INVALID_ARG, "rf_dgesv: need 1 <= n <= lda");
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return rf::fail(nullptr, RF_ERR_NO_DEVICE, "rf_dgesv: no such CUDA device");
+    }
+    // everything this call makes, released on every return path
+    struct Scope {
+        int prev;
+        cudaStream_t st = nullptr;
+        cublasHandle_t blas = nullptr;
+        double *dA = nullptr, *dx = nullptr;
+        int *dpiv = nullptr, *dinfo = nullptr;
+        ~Scope() {
+            if (st) cudaStreamSynchronize(st);
+            cudaFree(dA);
+            cudaFree(dx);
+            cudaFree(dpiv);
+            cudaFree(dinfo);
+            if (blas) cublasDestroy(blas);
+            if (st) cudaStreamDestroy(st);
+            cudaSetDevice(prev);
+        }
+    } sc{prev};
+    auto cuda = [](cudaError_t e, const char *what) {
+        cudaGetLastError();
+        return rf::fail(nullptr, e == cudaErrorMemoryAllocation ? RF_ERR_OOM : RF_ERR_CUDA,
+                        std::string("rf_dgesv: ") + what + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&sc.st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda(e, "stream");
+    const size_t nn = (size_t)n;
+    if ((e = cudaMalloc(&sc.dA, sizeof(double) * nn * nn)) != cudaSuccess) return cuda(e, "device copy of A");
+    if ((e = cudaMalloc(&sc.dx, sizeof(double) * nn)) != cudaSuccess ||
+        (e = cudaMalloc(&sc.dpiv, sizeof(int) * nn)) != cudaSuccess ||
+        (e = cudaMalloc(&sc.dinfo, sizeof(int))) != cudaSuccess)
+        return cuda(e, "device buffers");
+    if (cublasCreate(&sc.blas) != CUBLAS_STATUS_SUCCESS)
+        return rf::fail(nullptr, RF_ERR_CUDA, "rf_dgesv: cuBLAS handle could not be created");
+    if ((e = cudaMemcpy2DAsync(sc.dA, sizeof(double) * nn, A, sizeof(double) * (size_t)lda, sizeof(double) * nn, nn,
+                               cudaMemcpyHostToDevice, sc.st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(sc.dx, b, sizeof(double) * nn, cudaMemcpyHostToDevice, sc.st)) != cudaSuccess)
+        return cuda(e, "upload");
+    int64_t launches = 0;
+    if ((e = rf::lu_factor(sc.dA, n, n, sc.dpiv, sc.dinfo, sc.blas, sc.st, &launches)) != cudaSuccess)
+        return cuda(e, "LU factorisation");
+    int hinfo = 0;
+    if ((e = cudaMemcpyAsync(&hinfo, sc.dinfo, sizeof(int), cudaMemcpyDeviceToHost, sc.st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(sc.st)) != cudaSuccess)
+        return cuda(e, "LU factorisation");
+    *info = hinfo;
+    if (hinfo == 0) {
+        if ((e = rf::lu_solve(sc.dA, n, n, sc.dpiv, sc.dx, sc.st, &launches)) != cudaSuccess)
+            return cuda(e, "LU solve");
+        if ((e = cudaMemcpyAsync(x, sc.dx, sizeof(double) * nn, cudaMemcpyDeviceToHost, sc.st)) != cudaSuccess)
+            return cuda(e, "download");
+    }
+    if (ipiv) {
+        std::vector<int> hp(nn);
+        if ((e = cudaMemcpyAsync(hp.data(), sc.dpiv, sizeof(int) * nn, cudaMemcpyDeviceToHost, sc.st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(sc.st)) != cudaSuccess)
+            return cuda(e, "download");
+        for (size_t i = 0; i < nn; ++i) ipiv[i] = hp[i] + 1;
+    }
+    if ((e = cudaStreamSynchronize(sc.st)) != cudaSuccess) return cuda(e, "LU solve");
     return RF_OK;
 }
 

@@ -108,6 +108,19 @@ def test_direct_solver_needs_fp64():
     assert e.value.status == 1 and "RF_PREC_FP64" in str(e.value)
 
 
+def test_dgesv_rejects_bad_arguments():
+    """rf_dgesv checks its arguments before any device work."""
+    lib = L.lib()
+    A, b, x = np.eye(3), np.ones(3), np.zeros(3)
+    info = ctypes.c_int32(-1)
+    dp = ctypes.POINTER(ctypes.c_double)
+    Ap, bp, xp = (v.ctypes.data_as(dp) for v in (A, b, x))
+    assert lib.rf_dgesv(3, None, 3, bp, xp, None, ctypes.byref(info), 0) == 1  # RF_ERR_INVALID_ARG
+    assert lib.rf_dgesv(3, Ap, 2, bp, xp, None, ctypes.byref(info), 0) == 1  # RF_ERR_INVALID_ARG
+    assert lib.rf_dgesv(0, Ap, 3, bp, xp, None, ctypes.byref(info), 0) == 1  # RF_ERR_INVALID_ARG
+    assert b"rf_dgesv" in lib.rf_last_error(None)
+
+
 def test_create_without_gpu_fails_cleanly():
     from conftest import gpu_available
 

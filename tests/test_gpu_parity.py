@@ -101,6 +101,56 @@ def test_direct_solver_matches_oracle_lu(M):
     assert np.abs(x - x_o).max() <= 1e-10 * np.abs(x_o).max()
 
 
+def _dgesv(A, b, lda_pad=0):
+    """rf_dgesv through the C ABI on a host copy of A with lda = n + lda_pad."""
+    import ctypes
+
+    from rigidfibers_kth_b200 import _lib as L
+
+    n = len(b)
+    Ah = np.zeros((n + lda_pad, n), order="F")
+    Ah[:n, :] = A
+    Ah[n:, :] = np.nan  # rows past n must never be read
+    x = np.zeros(n)
+    piv = np.zeros(n, dtype=np.int32)
+    info = ctypes.c_int32(-1)
+    dp = ctypes.POINTER(ctypes.c_double)
+    st = L.lib().rf_dgesv(n, Ah.ctypes.data_as(dp), n + lda_pad, np.ascontiguousarray(b).ctypes.data_as(dp),
+                          x.ctypes.data_as(dp), piv.ctypes.data, ctypes.byref(info), 0)
+    L.check(st)
+    assert np.all(np.isnan(Ah[n:, :])) and np.array_equal(Ah[:n, :], A)  # A left unchanged
+    return x, piv, info.value
+
+
+def test_dgesv_general_matrix_pivots_like_lapack():
+    """The system matrices of fiber layouts are close to the identity and
+    need no row interchange, so the device LU's pivot search and swaps are
+    checked on general matrices: random N(0, 1) entries (a row interchange in
+    almost every column), n = 777 (the last 64-column panel and 8-column
+    sub-panel partial), padded leading dimension.  Pivots equal LAPACK's
+    (scipy's dgetrf, 1-based), x matches the oracle's LU to 1e-10 and the
+    backward error is at rounding level; a matrix with a zero column reports
+    LAPACK's info."""
+    import scipy.linalg as sl
+
+    rng = np.random.default_rng(777)
+    n = 777
+    A = rng.standard_normal((n, n))
+    b = rng.standard_normal(n)
+    x, piv, info = _dgesv(A, b, lda_pad=5)
+    assert info == 0
+    _, piv_ref = sl.lu_factor(A)
+    assert np.sum(piv_ref != np.arange(n)) > n // 2  # pivoting really happens
+    assert np.array_equal(piv, piv_ref + 1)
+    x_o = rfo.solve_direct(A, b)
+    assert np.abs(x - x_o).max() <= 1e-10 * np.abs(x_o).max()
+    assert np.linalg.norm(A @ x - b) / (np.linalg.norm(A) * np.linalg.norm(x)) <= 1e-14
+    A0 = A.copy()
+    A0[:, 100] = 0.0
+    _, _, info0 = _dgesv(A0, b)
+    assert info0 == 101
+
+
 def test_direct_solver_steps_match_gmres():
     """Three time steps with the LU and with GMRES at 1e-13 agree."""
     pos, ori = rf.generate_layout(200, "uniform", 4.0, 0.2, seed=1950)
