@@ -744,15 +744,17 @@ __global__ void __launch_bounds__(32 * RF_FAR_WARPS, RF_FAR_MINB / RF_FAR_WARPS)
 #pragma unroll 1
         for (int it = 0; it < N; ++it) {
             const int m = it < (N + 1) / 2 ? 2 * it + 1 : 2 * (it - (N + 1) / 2) + 2;
-            // the copy engine has read the previous weight's staged columns
-            if (lane < kCopyLanes) bulk_wait_read();
-            __syncwarp();
             float S[7][N + 1];
             if (m & 1) far_sets_reg<N, 1>(m, U, V, S);
             else far_sets_reg<N, 0>(m, U, V, S);
             // the block entries and panel rows: theta's 3 x 3 blocks with their
             // columns (components of X, Y, Z) paired on the packed FP32 units
             const V3p Dp = v3p(D), tp = v3p(t), pp3 = v3p(p);
+            // the copy engine has read the previous weight's staged columns
+            // (waited for only here, so that the coefficient sets above
+            // overlap the copies)
+            if (lane < kCopyLanes) bulk_wait_read();
+            __syncwarp();
             // row k = 0: velocity panel P0 only
             if (PANELS) {
                 V3p X, Y, Z;
