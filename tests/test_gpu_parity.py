@@ -151,6 +151,23 @@ def test_dgesv_general_matrix_pivots_like_lapack():
     assert info0 == 101
 
 
+@pytest.mark.parametrize("n", [1, 7, 8, 63, 64, 65, 130])
+def test_dgesv_panel_edges(n):
+    """Sizes at the edges of the 8-column sub-panels and 64-column panels
+    (one column, a partial sub-panel, exactly one sub-panel or panel, one
+    column more): pivots equal LAPACK's and x solves the system."""
+    import scipy.linalg as sl
+
+    rng = np.random.default_rng(1000 + n)
+    A = rng.standard_normal((n, n))
+    b = rng.standard_normal(n)
+    x, piv, info = _dgesv(A, b, lda_pad=3)
+    assert info == 0
+    assert np.array_equal(piv, sl.lu_factor(A)[1] + 1)
+    x_ref = np.linalg.solve(A, b)
+    assert np.abs(x - x_ref).max() <= 1e-10 * max(1.0, np.abs(x_ref).max())
+
+
 def test_direct_solver_steps_match_gmres():
     """Three time steps with the LU and with GMRES at 1e-13 agree."""
     pos, ori = rf.generate_layout(200, "uniform", 4.0, 0.2, seed=1950)
