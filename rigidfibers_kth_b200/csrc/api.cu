@@ -393,11 +393,36 @@ rf_status rf_create(const rf_params *p, const double *positions, const double *o
         CKC(dalloc(&h->A32, asz), "alloc A (FP32)");
         CKC(cudaMemset(h->A32, 0, asz * 4), "memset A");
     }
-    // assembly chunking: about 8 CTAs per SM in the grid (from the whole
-    // system's targets also for a row-block shard, so that its right-hand
-    // side sums the same source chunks in the same order)
+    // assembly chunking (from the whole system's targets also for a
+    // row-block shard, so that its right-hand side sums the same source
+    // chunks in the same order).  The FP64 assembly runs CTAs of 4 targets,
+    // 4 resident per SM, the velocity kernel CTAs of 8 targets, 2 per SM: in
+    // both the grid takes about rounds x sources per CTA, rounds =
+    // (M / 4) x chunks / (4 SMs' worth of slots).  From a first guess of
+    // about 8 CTAs of 8 targets per SM, the sources per CTA (within a factor
+    // 4 below, but not below 16, and 2 above) that minimise that product;
+    // ties: the larger share.  At M = 4000 on 148 SMs: 13 chunks of 308
+    // sources (22 rounds, the last one nearly full) instead of 3 of 1334
+    // (6 rounds, the sixth nearly empty).
     const int tiles = (M + 7) / 8;
-    int chunks = std::max(1, std::min(M, (h->sm_count * 8 + tiles - 1) / tiles));
+    const int c0 = std::max(1, std::min(M, (h->sm_count * 8 + tiles - 1) / tiles));
+    const int per0 = (M + c0 - 1) / c0;
+    const int64_t ctas_x = (M + 3) / 4, slots = 4 * (int64_t)h->sm_count;
+    int chunks = c0;
+    {
+        int64_t best_cost = -1;
+        int best_share = per0;
+        for (int per = std::max(std::min(per0, 16), per0 / 4); per <= 2 * per0 && per <= M; ++per) {
+            const int c = (M + per - 1) / per;
+            const int share = (M + c - 1) / c;
+            const int64_t cost = ((ctas_x * c + slots - 1) / slots) * share;
+            if (best_cost < 0 || cost < best_cost || (cost == best_cost && share > best_share)) {
+                best_cost = cost;
+                best_share = share;
+                chunks = c;
+            }
+        }
+    }
     h->asm_chunk = (M + chunks - 1) / chunks;
     h->asm_chunks = (M + h->asm_chunk - 1) / h->asm_chunk;
     h->vel_chunk = h->asm_chunk;
