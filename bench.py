@@ -103,7 +103,8 @@ def parse_args():
     ap.add_argument("--pc-damping", type=float, default=None,
                     help="damping of the preconditioner's coupling blocks (default: the library's)")
     ap.add_argument("--near-c", type=float, default=None,
-                    help="squared distance below which a pair's integrals stay FP64 (default: the library's)")
+                    help="squared distance below which a pair's integrals stay FP64 (default: the library's, 6; "
+                         "smaller values are raised to 6)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison arm")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--config", type=int, choices=[1, 2, 3, 4, 5], default=4,
